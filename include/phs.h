@@ -1,0 +1,183 @@
+/*
+ * phs.h -- C ABI of the B200 time-stepping and electrogram path of PyHeartSim.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point returns an
+ * int status (PHS_OK on success).  Device pointers are marked "device"; all
+ * other pointers are host memory.  Streams are passed as `void*` holding a
+ * cudaStream_t (NULL = the legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside jiyuehe/PyHeartSim):
+ *   simulation/simulation_gpu.py:261-409   compute(n_voxel, P_2d, geometry_data,
+ *                                           simulation_parameters, arrhythmia_parameters)
+ *   simulation/simulation_gpu.py:71-136    rk4_reaction_kernel / reaction_step_gpu_rk4
+ *   simulation/simulation_gpu.py:138-225   build_diffusion_matrix_gpu (replaced by a
+ *                                           matrix-free stencil on a compacted table)
+ *   simulation/simulation_gpu.py:227-259   crank_nicolson_diffusion_step_gpu (CuPy GMRES(50))
+ *   simulation/pacing.py:136-170           apply_pacing (compiled to a per-step schedule)
+ *   simulation/unipolar_electrogram_gpu.py:21-152  compute_egm_kernel_batched / compute
+ *   simulation/unipolar_electrogram_equation_parts.py:41-124  distances, gradients, normalisation
+ */
+#ifndef PHS_H
+#define PHS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define PHS_OK                 0
+#define PHS_ERR_BAD_ARG        1  /* invalid argument or size                       */
+#define PHS_ERR_BAD_TABLE      2  /* neighbour index out of range                    */
+#define PHS_WARN_NO_CONVERGE   3  /* a CN solve hit maxiter (reference prints a warning,
+                                     simulation/simulation_gpu.py:254-255)           */
+#define PHS_ERR_NONFINITE      4  /* NaN/Inf in a solver norm                         */
+#define PHS_ERR_OOM            5  /* device allocation failed                         */
+#define PHS_ERR_TIMEOUT        6  /* a bounded device-side wait gave up               */
+#define PHS_ERR_CUDA           7  /* other CUDA runtime error                         */
+#define PHS_ERR_UNSUPPORTED    8  /* input the build does not handle                  */
+#define PHS_ERR_STATE          9  /* call not valid in the current state              */
+
+#define PHS_MODEL_MS 0           /* Mitchell-Schaeffer (heart_model_flag 0)            */
+#define PHS_MODEL_AP 1           /* Aliev-Panfilov     (heart_model_flag 1)            */
+
+#define PHS_PREC_F32 32          /* FP32 state/basis, FP64 dots and norms              */
+#define PHS_PREC_F64 64          /* FP64 everywhere (plain drop-in form)               */
+
+#define PHS_VFLAG_S1      1u     /* voxel is in the S1 pacing set                      */
+#define PHS_VFLAG_S2      2u     /* voxel is in the S2 pacing set                      */
+#define PHS_VFLAG_TBLOCK  4u     /* voxel row is zeroed while the temporary block holds */
+
+#define PHS_EGM_F64    0         /* FP64 contraction (plain drop-in form)              */
+#define PHS_EGM_BF16X3 1         /* BF16 hi/lo split, 3 tcgen05 products, FP32 accumulate */
+
+const char* phs_status_string(int status);
+int phs_version(void);
+/* SM count and resident CTAs per SM of the step kernel for a precision. */
+int phs_device_query(int precision, int* sm_count, int* ctas_per_sm);
+/* Last CUDA error text recorded by the library (static storage). */
+const char* phs_last_error(void);
+
+/* ------------------------------------------------------- one instance
+ * A simulation instance, compacted and ready to upload.  Built on the host from
+ * the reference's inputs (P_2d, neighbor_id_2d, the parameter dicts).          */
+typedef struct phs_instance_desc {
+    int64_t n_voxel;
+    int32_t model;            /* PHS_MODEL_MS / PHS_MODEL_AP                              */
+    int32_t restart;          /* GMRES restart length m (reference: 50), 1..50            */
+    const int32_t* nb6;       /* [n][6] neighbours +x,-x,+y,-y,+z,-z; absent (-1) -> 0 as in the reference */
+    const double* coef6;      /* [n][6] c_n/(4 Delta^2) * P_2d[n,k]  (permanent block: 0)   */
+    const uint8_t* vflags;    /* [n] PHS_VFLAG_* bits                                       */
+    const double* vparams;    /* [n][5] P_2d[:,15:20], or NULL to use params[]              */
+    double params[5];         /* MS: tau_open, tau_close, tau_in, tau_out, v_gate;
+                                 AP: k, a, eps0, mu1, mu2 (P_2d columns 15..19)             */
+    double dt;                /* model time step                                            */
+    double j_stim;            /* stimulus magnitude (reference: 1)                          */
+    int64_t n_steps;          /* steps to run: int(round(t_final/dt))                       */
+    const uint8_t* stim;      /* [n_steps] bit0: S1 window active, bit1: S2 window active   */
+    int64_t tblock_steps;     /* steps 0..tblock_steps-1 use the temporary-block operator   */
+    int32_t sample_stride;    /* sample after step s when s % stride == 0 (0: every step)   */
+    int32_t n_samples;        /* history length S                                           */
+    int32_t save_h;           /* also keep the gate history                                 */
+    int32_t full_cycles;      /* 1: CuPy GMRES semantics (full restart cycles, true-residual
+                                 test at each cycle start); 0: Givens early exit            */
+    double u0, h0;            /* initial state (MS: 0,1; AP: 0,0)                           */
+    double tol, atol;         /* stop when ||r|| <= max(atol, tol*||b||)                    */
+    int32_t maxiter;          /* Arnoldi steps per solve before giving up (reference 10000) */
+    int32_t _reserved;
+} phs_instance_desc;
+
+/* Per-instance progress and solver statistics. */
+typedef struct phs_instance_info {
+    int64_t n_voxel;
+    int64_t step;             /* steps completed                                   */
+    int64_t n_steps;
+    int32_t samples;          /* history samples written                           */
+    int32_t status;           /* PHS_OK / PHS_WARN_NO_CONVERGE / PHS_ERR_NONFINITE  */
+    int64_t arnoldi_steps;    /* total Arnoldi iterations                          */
+    int64_t solves;           /* CN solves that iterated                           */
+    int32_t max_arnoldi;      /* most Arnoldi iterations in one solve              */
+    int32_t nonconverged;     /* solves that stopped on maxiter                    */
+} phs_instance_info;
+
+/* ------------------------------------------------ batched engine
+ * An engine owns device memory for any number of instances of one precision and
+ * advances all active instances with one persistent launch per call.            */
+typedef struct phs_engine phs_engine;
+
+int phs_engine_create(int precision, phs_engine** out);
+int phs_engine_destroy(phs_engine* eng);
+/* Upload an instance; returns its slot. */
+int phs_instance_add(phs_engine* eng, const phs_instance_desc* desc, int* slot);
+int phs_instance_remove(phs_engine* eng, int slot);
+int phs_instance_info_get(phs_engine* eng, int slot, phs_instance_info* info);
+/* Advance every unfinished instance by up to n_steps steps (one persistent launch,
+ * or one per wave when waves > 1).  ctas_per_sm 0 = occupancy limit.  Returns the
+ * worst instance status; the launch is asynchronous unless sync != 0.           */
+int phs_engine_advance(phs_engine* eng, int64_t n_steps, int ctas_per_sm, void* stream, int sync);
+/* Copy history samples [s0, s0+count) of a slot to host buffers ([count][n],
+ * element type = engine precision; h_dst may be NULL).  Synchronous.           */
+int phs_instance_read_history(phs_engine* eng, int slot, int32_t s0, int32_t count,
+                              void* u_dst, void* h_dst);
+/* Copy the current state u, h ([n] each, engine precision) and the activation
+ * step table lat ([n] int32, -1 = not activated) to host.  Any may be NULL.    */
+int phs_instance_read_state(phs_engine* eng, int slot, void* u_dst, void* h_dst, int32_t* lat_dst);
+/* Device pointers of an instance's state (for device-side consumers). */
+int phs_instance_device_ptrs(phs_engine* eng, int slot, void** u, void** hist_u, int32_t** lat);
+/* Number of kernel launches the engine issued since creation. */
+int64_t phs_engine_launch_count(phs_engine* eng);
+
+/* ------------------------------------------- one-shot drop-in (host buffers)
+ * Runs a whole instance: upload, all steps, download.  Replaces
+ * simulation/simulation_gpu.py:261-409.  u_hist/h_hist: [n_samples][n] host,
+ * element type = precision.  *n_saved receives the samples written.            */
+int phs_simulate(const phs_instance_desc* desc, int precision, void* u_hist, void* h_hist,
+                 int32_t* lat, int32_t* n_saved, phs_instance_info* info);
+
+/* ------------------------------------------------------------ electrogram
+ * Lead field: M[w][e] such that egm[t][e] = sum_w V[t][w] * M[w][e] reproduces
+ * simulation/unipolar_electrogram_gpu.py:55-69 with the gradients of
+ * simulation/unipolar_electrogram_equation_parts.py:60-103 folded in.
+ * Output is stored transposed, Mt[e][w] (K-major), FP64, on the device.
+ *   voxel_xyz  device [n_v][3] f64      electrode_xyz device [n_e][3] f64
+ *   c_voxel    device [n_v] f64         D0 device [n_v][9] f64 row-major, or NULL (identity)
+ *   in_ptr     device [n_v+1] int32     CSR of incoming gradient terms per voxel w
+ *   in_src     device [nnz] int32       source voxel v of each term
+ *   in_dir     device [nnz] int8        +(d+1) or -(d+1), d = 0,1,2 (x,y,z)          */
+int phs_egm_leadfield_f64(int64_t n_v, int64_t n_e, const double* voxel_xyz,
+                          const double* electrode_xyz, const double* c_voxel, const double* D0,
+                          const int32_t* in_ptr, const int32_t* in_src, const int8_t* in_dir,
+                          double inv_two_delta, double* Mt, void* stream);
+/* egm[t][e] = sum_w V[t][w] Mt[e][w], FP64 (device pointers). */
+int phs_egm_contract_f64(int64_t T, int64_t n_v, int64_t n_e, const double* V, int64_t ldv,
+                         const double* Mt, double* egm, void* stream);
+/* Split an FP64/FP32 matrix (rows x cols, leading dim ld) into BF16 hi and lo parts,
+ * written with leading dimension ld_out (zero padding to ld_out).  src_is_f64 selects
+ * the source type.                                                               */
+int phs_split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, int src_is_f64,
+                   uint16_t* hi, uint16_t* lo, int64_t rows_out, int64_t ld_out, void* stream);
+/* egm[t][e] = sum_w (Vhi Mhi + Vhi Mlo + Vlo Mhi) on the tcgen05 tensor cores,
+ * FP32 accumulation in TMEM, split-K partials reduced in a fixed order.
+ * Vhi/Vlo: [T_pad][K_pad] bf16; Mhi/Mlo: [n_e_pad][K_pad] bf16 (device).
+ * T_pad % 128 == 0, n_e_pad % 128 == 0, K_pad % 64 == 0.  work: device scratch
+ * of phs_egm_bf16x3_workspace() bytes.                                            */
+int64_t phs_egm_bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
+int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
+                            const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi,
+                            const uint16_t* Mlo, float* egm, void* work, void* stream);
+/* Scale egm ([T][n_e], f64 or f32 per is_f64) in place by 1/mean_e(max_t - min_t),
+ * simulation/unipolar_electrogram_equation_parts.py:118-124.                      */
+int phs_egm_normalize(int64_t T, int64_t n_e, void* egm, int is_f64, void* stream);
+
+/* One-shot drop-in for simulation/unipolar_electrogram_gpu.py:71-152 with host
+ * buffers: V [T][n_v] f64, tables as above (host), egm_out [T][n_e] f64. */
+int phs_electrogram(int64_t T, int64_t n_v, int64_t n_e, const double* V, const double* voxel_xyz,
+                    const double* electrode_xyz, const double* c_voxel, const double* D0,
+                    const int32_t* in_ptr, const int32_t* in_src, const int8_t* in_dir,
+                    double delta, int mode, double* egm_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHS_H */

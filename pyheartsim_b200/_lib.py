@@ -1,0 +1,199 @@
+"""ctypes binding of ``libphs.so`` (the C ABI declared in include/phs.h).
+
+The library is built in-tree by ``pyheartsim_b200.build``.  There is no
+fallback: if the library is missing every call raises, so a missing CUDA
+extension can never be mistaken for a working one.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libphs.so")
+
+PHS_OK = 0
+PHS_ERR_BAD_ARG = 1
+PHS_ERR_BAD_TABLE = 2
+PHS_WARN_NO_CONVERGE = 3
+PHS_ERR_NONFINITE = 4
+PHS_ERR_OOM = 5
+PHS_ERR_TIMEOUT = 6
+PHS_ERR_CUDA = 7
+PHS_ERR_UNSUPPORTED = 8
+PHS_ERR_STATE = 9
+
+PREC_F32 = 32
+PREC_F64 = 64
+EGM_F64 = 0
+EGM_BF16X3 = 1
+
+VFLAG_S1 = 1
+VFLAG_S2 = 2
+VFLAG_TBLOCK = 4
+
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_uint8_p = ctypes.POINTER(ctypes.c_uint8)
+c_uint16_p = ctypes.POINTER(ctypes.c_uint16)
+c_int8_p = ctypes.POINTER(ctypes.c_int8)
+c_float_p = ctypes.POINTER(ctypes.c_float)
+
+
+class InstanceDesc(ctypes.Structure):
+    """Mirror of ``phs_instance_desc``."""
+    _fields_ = [
+        ("n_voxel", ctypes.c_int64),
+        ("model", ctypes.c_int32),
+        ("restart", ctypes.c_int32),
+        ("nb6", c_int32_p),
+        ("coef6", c_double_p),
+        ("vflags", c_uint8_p),
+        ("vparams", c_double_p),
+        ("params", ctypes.c_double * 5),
+        ("dt", ctypes.c_double),
+        ("j_stim", ctypes.c_double),
+        ("n_steps", ctypes.c_int64),
+        ("stim", c_uint8_p),
+        ("tblock_steps", ctypes.c_int64),
+        ("sample_stride", ctypes.c_int32),
+        ("n_samples", ctypes.c_int32),
+        ("save_h", ctypes.c_int32),
+        ("full_cycles", ctypes.c_int32),
+        ("u0", ctypes.c_double),
+        ("h0", ctypes.c_double),
+        ("tol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("maxiter", ctypes.c_int32),
+        ("_reserved", ctypes.c_int32),
+    ]
+
+
+class InstanceInfo(ctypes.Structure):
+    """Mirror of ``phs_instance_info``."""
+    _fields_ = [
+        ("n_voxel", ctypes.c_int64),
+        ("step", ctypes.c_int64),
+        ("n_steps", ctypes.c_int64),
+        ("samples", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("arnoldi_steps", ctypes.c_int64),
+        ("solves", ctypes.c_int64),
+        ("max_arnoldi", ctypes.c_int32),
+        ("nonconverged", ctypes.c_int32),
+    ]
+
+
+# name -> (restype, argtypes); every symbol of include/phs.h
+SIGNATURES = {
+    "phs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "phs_version": (ctypes.c_int, []),
+    "phs_device_query": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "phs_last_error": (ctypes.c_char_p, []),
+    "phs_engine_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "phs_engine_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "phs_instance_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_int)]),
+    "phs_instance_remove": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "phs_instance_info_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(InstanceInfo)]),
+    "phs_engine_advance": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
+    "phs_instance_read_history": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_instance_read_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                               c_int32_p]),
+    "phs_instance_device_ptrs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(c_int32_p)]),
+    "phs_engine_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "phs_simulate": (ctypes.c_int, [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                    c_int32_p, c_int32_p, ctypes.POINTER(InstanceInfo)]),
+    "phs_egm_leadfield_f64": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_egm_contract_f64": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                            ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_split_bf16": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.c_void_p]),
+    "phs_egm_bf16x3_workspace": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]),
+    "phs_egm_contract_bf16x3": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_egm_normalize": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p]),
+    "phs_electrogram": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_double_p, c_double_p,
+                                       c_double_p, c_double_p, c_double_p, c_int32_p, c_int32_p, c_int8_p,
+                                       ctypes.c_double, ctypes.c_int, c_double_p]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class PhsError(RuntimeError):
+    """A C-ABI call returned an error status."""
+
+    def __init__(self, status, where):
+        self.status = status
+        msg = status_string(status)
+        detail = ""
+        try:
+            detail = lib().phs_last_error().decode()
+        except Exception:
+            pass
+        super().__init__(f"{where}: {msg} (status {status}){'; ' + detail if detail else ''}")
+
+
+def lib():
+    """Load libphs.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pyheartsim_b200.build` "
+                                   "(the CUDA path has no fallback)")
+            h = ctypes.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(h, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = h
+    return _lib
+
+
+def status_string(status):
+    try:
+        return lib().phs_status_string(int(status)).decode()
+    except Exception:
+        return f"status {status}"
+
+
+def check(status, where, allow_warn=False):
+    """Raise PhsError unless ``status`` is OK (or the no-convergence warning when allowed)."""
+    if status == PHS_OK or (allow_warn and status == PHS_WARN_NO_CONVERGE):
+        return status
+    raise PhsError(status, where)
+
+
+def ptr(a, ctype):
+    """ctypes pointer to a C-contiguous numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def vptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    assert a.flags["C_CONTIGUOUS"]
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def np_dtype(precision):
+    return np.float64 if precision == PREC_F64 else np.float32

@@ -1,0 +1,157 @@
+"""Compile the reference's inputs into one device instance (``phs_instance_desc``).
+
+Input is exactly what ``simulation/simulation_gpu.py::compute`` receives:
+``n_voxel``, ``P_2d`` (n, 21), ``geometry_data`` ({'neighbor_id_2d', 'Delta'}),
+``simulation_parameters`` and ``arrhythmia_parameters``.  The reference builds a
+CSR Laplacian with a Python loop (simulation/simulation_gpu.py:138-225); here the
+same operator is kept matrix-free as a compacted table:
+
+* ``nb6[n, k]``   the six face neighbours, ``-1`` remapped to 0 exactly as the
+                  reference does before building L (simulation_gpu.py:296-297);
+* ``coef6[n, k]`` ``P_2d[n,20] / (4 Delta^2) * P_2d[n,k]`` with the permanent
+                  block (node_flag == 4) applied to column 20 (simulation_gpu.py:312-313);
+* ``vflags[n]``   S1 / S2 membership and the temporary block (node_flag == 3);
+
+so ``(L u)[n] = sum_k coef6[n,k] * (u[nb6[n,k]] - u[n])`` is the reference's
+row n (its diagonal is minus the sum of the neighbour entries).
+"""
+import numpy as np
+
+from . import _lib
+from .simulation import pacing
+
+
+class CompiledInstance:
+    """Host arrays + scalars of one instance, and the ctypes descriptor over them."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+        self._desc = None
+
+    def desc(self):
+        """ctypes ``phs_instance_desc`` referencing this object's arrays (keep self alive)."""
+        d = _lib.InstanceDesc()
+        d.n_voxel = self.n_voxel
+        d.model = self.model
+        d.restart = self.restart
+        d.nb6 = _lib.ptr(self.nb6, _lib.ctypes.c_int32)
+        d.coef6 = _lib.ptr(self.coef6, _lib.ctypes.c_double)
+        d.vflags = _lib.ptr(self.vflags, _lib.ctypes.c_uint8)
+        d.vparams = _lib.ptr(self.vparams, _lib.ctypes.c_double) if self.vparams is not None else None
+        for i in range(5):
+            d.params[i] = float(self.params[i])
+        d.dt = self.dt
+        d.j_stim = self.j_stim
+        d.n_steps = self.n_steps
+        d.stim = _lib.ptr(self.stim, _lib.ctypes.c_uint8)
+        d.tblock_steps = self.tblock_steps
+        d.sample_stride = self.sample_stride
+        d.n_samples = self.n_samples
+        d.save_h = self.save_h
+        d.full_cycles = self.full_cycles
+        d.u0 = self.u0
+        d.h0 = self.h0
+        d.tol = self.tol
+        d.atol = self.atol
+        d.maxiter = self.maxiter
+        self._desc = d
+        return d
+
+    def sample_times(self, n_saved):
+        """physical_time of the first ``n_saved`` samples: the sample taken after
+        step k is stamped ``k * dt * time_scale`` (simulation_gpu.py:395-407)."""
+        if self.sample_stride > 0:
+            steps = np.arange(n_saved, dtype=np.int64) * self.sample_stride
+        else:
+            steps = np.arange(n_saved, dtype=np.int64)
+        return (steps.astype(np.float64) * self.dt) * self.time_scale
+
+
+def step_counts(simulation_parameters):
+    """(n_steps, n_samples, stride), simulation/simulation_gpu.py:286-290, 355-356."""
+    t_final = float(simulation_parameters['t_final'])
+    dt = simulation_parameters['dt']
+    ts = simulation_parameters['time_scale']
+    if simulation_parameters['heart_model_flag'] == 0:
+        n_samples = int(np.round(t_final))
+    else:
+        n_samples = int(np.round(t_final * ts))
+    n_steps = int(np.round(t_final / dt))
+    stride = int(1 / (dt * ts))
+    return n_steps, n_samples, stride
+
+
+def tblock_steps(n_steps, dt):
+    """Steps run with the temporary-block operator: model_time = step*dt in
+    [0, 350*dt) (simulation/simulation_gpu.py:365-370)."""
+    t = np.arange(n_steps, dtype=np.float64) * dt
+    on = (t >= 0) & (t < 350 * dt)
+    k = int(on.sum())
+    if k and not on[:k].all():
+        raise AssertionError("temporary block window is not a prefix of the run")
+    return k
+
+
+def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
+                     full_cycles=True, tol=1e-5, atol=1e-5, restart=50, maxiter=10000,
+                     pacing_duration=None, save_h=True, max_steps=None):
+    """Build a :class:`CompiledInstance` with the reference's semantics.
+
+    ``full_cycles=True`` keeps CuPy's GMRES(restart) behaviour (the plain
+    drop-in); ``False`` stops each solve as soon as the Givens residual
+    estimate meets the same tolerance.
+    """
+    n = int(n_voxel)
+    P = np.asarray(P_2d, dtype=np.float64)
+    if P.shape != (n, 21):
+        raise ValueError(f"P_2d must be ({n}, 21), got {P.shape}")
+    nb = np.asarray(geometry_data['neighbor_id_2d'])
+    if nb.ndim != 2 or nb.shape[0] != n or nb.shape[1] < 6:
+        raise ValueError("neighbor_id_2d must be (n_voxel, 18)")
+    if np.any(nb[:, :6] < -1) or np.any(nb[:, :6] >= n):
+        raise ValueError("neighbor_id_2d holds indices outside [-1, n_voxel)")
+    if np.any(P[:, 6:15] != 0):
+        raise NotImplementedError("anisotropic cross terms (P_2d columns 6..14 non-zero) are not "
+                                  "supported by this build; the reference's load_fiber always gives "
+                                  "D0 = I, for which they are zero")
+    Delta = float(geometry_data['Delta'])
+    model = int(simulation_parameters['heart_model_flag'])
+    if model not in (0, 1):
+        raise ValueError("heart_model_flag must be 0 (Mitchell-Schaeffer) or 1 (Aliev-Panfilov)")
+    flag = simulation_parameters['arrhythmia_flag']
+    dt = simulation_parameters['dt']
+    ts = simulation_parameters['time_scale']
+    node_flag = np.asarray(arrhythmia_parameters['node_flag'])
+
+    n_steps, n_samples, stride = step_counts(simulation_parameters)
+    if max_steps is not None:
+        n_steps = min(n_steps, int(max_steps))
+    s1, s2, s1_t, jmag, pdur, s2_t = pacing.assign_pacing_parameters(
+        arrhythmia_parameters, flag, simulation_parameters, pacing_duration)
+    stim = pacing.schedule(n_steps, dt, arrhythmia_parameters, simulation_parameters, flag, s1_t, pdur, s2_t)
+
+    c = P[:, 20].copy()
+    c[node_flag == 4] = 0.0                       # permanent block
+    nb6 = nb[:, :6].astype(np.int64).copy()
+    nb6[nb6 == -1] = 0                            # the reference's -1 -> 0 remap
+    coef6 = (c / (4 * Delta ** 2))[:, None] * P[:, :6]
+    vflags = np.zeros(n, dtype=np.uint8)
+    s1 = np.atleast_1d(np.asarray(s1, dtype=np.int64)) if np.size(s1) else np.zeros(0, np.int64)
+    s2 = np.atleast_1d(np.asarray(s2, dtype=np.int64)) if np.size(s2) else np.zeros(0, np.int64)
+    vflags[s1] |= _lib.VFLAG_S1
+    vflags[s2] |= _lib.VFLAG_S2
+    vflags[node_flag == 3] |= _lib.VFLAG_TBLOCK
+    tb = tblock_steps(n_steps, dt) if np.any(node_flag == 3) else 0
+
+    mp = P[:, 15:20]
+    uniform = bool(np.all(mp == mp[0:1]))
+    params = mp[0].copy() if n else np.zeros(5)
+    vparams = None if uniform else np.ascontiguousarray(mp)
+    u0, h0 = (0.0, 1.0) if model == 0 else (0.0, 0.0)
+    return CompiledInstance(
+        n_voxel=n, model=model, restart=int(min(restart, 50)), nb6=np.ascontiguousarray(nb6, dtype=np.int32),
+        coef6=np.ascontiguousarray(coef6), vflags=vflags, vparams=vparams, params=params, dt=float(dt),
+        j_stim=float(jmag), n_steps=int(n_steps), stim=np.ascontiguousarray(stim, dtype=np.uint8),
+        tblock_steps=int(tb), sample_stride=int(stride), n_samples=int(n_samples), save_h=int(bool(save_h)),
+        full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol), atol=float(atol),
+        maxiter=int(maxiter), time_scale=ts, Delta=Delta)

@@ -1,0 +1,24 @@
+"""Load the golden fixtures (tests/golden/*.npz, produced by running the
+reference's own code, see tests/golden/make_golden.py) as reference-style
+argument dicts."""
+import glob
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    g = np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False)
+    sp = {k[3:]: g[k].item() for k in g.files if k.startswith("sp_")}
+    ap = {k[3:]: g[k].item() for k in g.files if k.startswith("ap_")}
+    ap["s1_pacing_voxel_id"] = g["s1"]
+    ap["s2_pacing_voxel_id"] = g["s2"]
+    ap["node_flag"] = g["node_flag"]
+    geom = {"neighbor_id_2d": g["neighbor_id_2d"], "Delta": float(g["Delta"]), "voxel": g["voxel"]}
+    return dict(n=g["voxel"].shape[0], P_2d=g["P_2d"], geom=geom, sp=sp, ap=ap, g=g)

@@ -1,0 +1,125 @@
+"""Host-side compilation of the reference's inputs, checked against the oracle
+(no GPU)."""
+import numpy as np
+import pytest
+
+from oracle import egm_fp64, simulation_fp64
+from pyheartsim_b200 import instance
+from pyheartsim_b200.simulation import pacing, unipolar_electrogram_gpu
+from tests import golden_cases
+
+
+def _ref_windows(ap, sp, flag, n_steps, dt, s1_t, pdur, s2_t):
+    out = np.zeros(n_steps, dtype=np.uint8)
+    for k in range(n_steps):
+        a, b = simulation_fp64.pacing_windows(ap, sp, flag, k * dt, s1_t, pdur, s2_t)
+        out[k] = (1 if a else 0) | (2 if b else 0)
+    return out
+
+
+@pytest.mark.parametrize("flag", [0, 1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("model", [0, 1])
+def test_pacing_schedule_matches_reference_windows(flag, model):
+    ts = 1 if model == 0 else 6
+    sp = {"heart_model_flag": model, "time_scale": ts, "dt": 0.05 / ts, "t_final": 400 / ts}
+    ap = {"pacing_start_time": 10 / ts, "pacing_cycle_length": 37.3 / ts, "s1_t": 3.0 / ts,
+          "s1_s2_delta_t": 41.7 / ts, "s1_pacing_voxel_id": [0], "s2_pacing_voxel_id": [1]}
+    s1, s2, s1_t, jm, pdur, s2_t = pacing.assign_pacing_parameters(ap, flag, sp)
+    n = 8000
+    got = pacing.schedule(n, sp["dt"], ap, sp, flag, s1_t, pdur, s2_t)
+    want = _ref_windows(ap, sp, flag, n, sp["dt"], s1_t, pdur, s2_t)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_zero_cycle_length_raises_instead_of_hanging():
+    sp = {"heart_model_flag": 0, "time_scale": 1}
+    ap = {"pacing_start_time": 0.0, "pacing_cycle_length": 0.0}
+    with pytest.raises(ValueError):
+        pacing.schedule(100, 0.5, ap, sp, 0, 0.0, 5, 0.0)
+
+
+@pytest.mark.parametrize("t_final,dt,model", [(500, 0.05, 0), (1000 / 6, 0.02 / 6, 1), (12, 0.7, 0), (3, 2.0, 0)])
+def test_step_counts_match_reference(t_final, dt, model):
+    sp = {"t_final": t_final, "dt": dt, "heart_model_flag": model, "time_scale": 1 if model == 0 else 6}
+    assert instance.step_counts(sp) == simulation_fp64.step_schedule(sp)
+
+
+@pytest.mark.parametrize("name", golden_cases.names())
+def test_matrix_free_operator_equals_reference_csr(name):
+    c = golden_cases.load(name)
+    inst = instance.compile_instance(c["n"], c["P_2d"], c["geom"], c["sp"], c["ap"])
+    P = np.array(c["P_2d"], dtype=np.float64)
+    nf = np.asarray(c["ap"]["node_flag"])
+    P[nf == 4, 20] = 0.0
+    L = simulation_fp64.laplacian(P, c["geom"]["neighbor_id_2d"], c["geom"]["Delta"])
+    rng = np.random.default_rng(0)
+    for _ in range(3):
+        u = rng.standard_normal(c["n"])
+        mf = (inst.coef6 * (u[inst.nb6] - u[:, None])).sum(axis=1)
+        np.testing.assert_allclose(mf, L @ u, rtol=1e-12, atol=1e-12)
+    # temporary block rows
+    tb = (inst.vflags & 4) != 0
+    np.testing.assert_array_equal(tb, nf == 3)
+
+
+def test_incoming_gradient_terms_reproduce_leadfield():
+    c = golden_cases.load("slab_ap_flag1")
+    g = c["g"]
+    nb = g["neighbor_id_2d"]
+    el = g["egm_electrode_xyz"]
+    M_ref = egm_fp64.leadfield(el, g["voxel"], None, g["P_2d"][:, 20], float(g["Delta"]), nb)
+    ptr, src, dirs = unipolar_electrogram_gpu.incoming_gradient_terms(nb)
+    # numpy emulation of the gather the device kernel performs
+    n_v, n_e = g["voxel"].shape[0], el.shape[0]
+    M = np.zeros((n_v, n_e))
+    for w in range(n_v):
+        for q in range(ptr[w], ptr[w + 1]):
+            v, dd = src[q], dirs[q]
+            d = abs(dd) - 1
+            l = g["voxel"][v] - el
+            ln = np.maximum(np.linalg.norm(l, axis=1), 1.0)
+            gval = g["P_2d"][v, 20] / ln ** 3 * l[:, d] / (2 * float(g["Delta"]))
+            M[w] += gval if dd > 0 else -gval
+    np.testing.assert_allclose(M, M_ref, rtol=1e-12, atol=1e-14)
+
+
+def test_compile_rejects_bad_tables():
+    c = golden_cases.load("sheet_ms_flag4")
+    geom = dict(c["geom"])
+    nb = geom["neighbor_id_2d"].copy()
+    nb[3, 0] = c["n"] + 5
+    geom["neighbor_id_2d"] = nb
+    with pytest.raises(ValueError):
+        instance.compile_instance(c["n"], c["P_2d"], geom, c["sp"], c["ap"])
+    P = c["P_2d"].copy()
+    P[0, 9] = 0.5
+    with pytest.raises(NotImplementedError):
+        instance.compile_instance(c["n"], P, c["geom"], c["sp"], c["ap"])
+
+
+@pytest.mark.parametrize("name", golden_cases.names())
+def test_lattice_neighbors_and_P2d_match_reference(name):
+    from pyheartsim_b200 import geometry
+    c = golden_cases.load(name)
+    g = c["g"]
+    nb = geometry.lattice_neighbors(g["ijk"])
+    np.testing.assert_array_equal(nb, g["neighbor_id_2d"])     # utility/voxelization.py convention
+    n = c["n"]
+    par = {"c_voxel": g["P_2d"][:, 20]}
+    keys = (("tau_open_voxel", "tau_close_voxel", "tau_in_voxel", "tau_out_voxel", "v_gate_voxel")
+            if c["sp"]["heart_model_flag"] == 0 else
+            ("k_voxel", "a_voxel", "epsilon_0_voxel", "mu1_voxel", "mu2_voxel"))
+    for col, k in zip(range(15, 20), keys):
+        par[k] = g["P_2d"][:, col]
+    P = geometry.heart_model_equation_parts(c["sp"], n, geometry.load_fiber(n), nb, par)
+    np.testing.assert_array_equal(P, g["P_2d"])
+
+
+def test_shell_generator_is_seeded_and_sized():
+    from pyheartsim_b200 import synthetic
+    a = synthetic.shell(seed=0)
+    b = synthetic.shell(seed=0)
+    np.testing.assert_array_equal(a, b)
+    assert 60_000 < a.shape[0] < 130_000
+    nb = synthetic.lattice_neighbors(a) if hasattr(synthetic, "lattice_neighbors") else None
+    assert nb is not None and nb.shape == (a.shape[0], 18)
