@@ -24,6 +24,7 @@ def small_shell_ms(seed=1, t_phys=40.0, dt=0.05, scar_cov=0.15):
     from pyheartsim_b200.geometry import lattice_neighbors
     nb = lattice_neighbors(ijk)
     c = synthetic.scar(ijk, nb, scar_cov, rng)
-    s1 = [int(rng.integers(0, ijk.shape[0]))]
-    s1 = np.unique(np.concatenate([s1, nb[s1[0], :6][nb[s1[0], :6] >= 0]]))
+    healthy = np.where(c == 1.0)[0]
+    centre = ijk[healthy[int(rng.integers(0, healthy.size))]]
+    s1 = np.where(np.sum((ijk - centre) ** 2, axis=1) <= 9)[0]
     return synthetic.make_case(ijk, 0.4, 0, dt, t_phys, s1, flag=4, c_scale=c), 2.0
