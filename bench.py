@@ -1,0 +1,415 @@
+#!/usr/bin/env python3
+"""Benchmark of the PyHeartSim B200 hot path.
+
+Metric: voxel-steps/s of the batched FP32 engine (one voxel advanced by one dt,
+reaction + Crank-Nicolson diffusion) on the batched configuration: 64 seeded
+shells with 50k-400k voxels each (log-uniform, ~10.9M voxels), scar, focal
+pacing, half Mitchell-Schaeffer / half Aliev-Panfilov.  One bench "step" is
+one dt for every instance.  Inputs (10.9M voxels x ~160 B of state and
+solver workspace, ~1.7 GB) are larger than the 126 MB L2, so no flush is
+needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W]      # this build (B200)
+    python bench.py --impl reference                     # CPU port of the reference's stepper
+
+Under torchrun each rank runs its own batch (seeds offset by rank: weak
+scaling, no data-path collective); the timed region is bracketed by a barrier
+and the MAX over ranks is reported.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
+WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=40)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--steps-per-launch", type=int, default=10)
+    p.add_argument("--pre-steps", type=int, default=1000,
+                   help="steps run before warm-up so the timed window covers propagating fronts")
+    p.add_argument("--instances", type=int, default=64)
+    p.add_argument("--n-min", type=int, default=50_000)
+    p.add_argument("--n-max", type=int, default=400_000)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--tol", type=float, default=1e-7)
+    p.add_argument("--t-phys", type=float, default=500.0, help="simulated ms per instance")
+    p.add_argument("--no-extras", action="store_true", help="skip e2e, plain-FP64, accuracy and CPU legs")
+    p.add_argument("--no-tune", action="store_true", help="use the default step-kernel variant")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        out.update(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=reasons, samples=len(rows))
+        return out
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "of measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's CPU stepper (port of legacy/compute_simulation_cpu.py)
+    on one instance of the batch, on all host cores."""
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    from oracle import legacy_cpu
+    from pyheartsim_b200 import workloads
+    sizes = workloads.batch_sizes(args.instances, args.n_min, args.n_max, args.seed)
+    i = int(np.argsort(sizes[0::2])[len(sizes[0::2]) // 2]) * 2       # median Mitchell-Schaeffer instance
+    _, ref_args, meta = workloads.shell_case(i, int(sizes[i]), args.seed, tol=args.tol)
+    run = legacy_cpu.LegacyRun(*ref_args, pacing_duration=meta["pacing_ms"])
+    for _ in range(max(args.warmup, 3)):
+        run.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run.step()
+    dt = time.perf_counter() - t0
+    v = meta["n"] * args.steps / dt
+    cores = legacy_cpu.threads()
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "voxel-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": f"instance {i} ({meta['n']} voxels, Mitchell-Schaeffer)",
+                       "solver": "legacy RK4 (numba parallel) + SciPy BiCGSTAB atol 1e-6"},
+            "cpu_baseline": {"value": v, "unit": "voxel-steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} steps of instance {i} ({meta['n']} voxels)"},
+            "e2e": {"value": v, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- this build
+def run_b200(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    from pyheartsim_b200 import _lib, roofline, workloads
+    from pyheartsim_b200.engine import BatchedEngine
+
+    seed = args.seed + 7919 * rank
+    batch = workloads.batched_shells(args.instances, args.n_min, args.n_max, seed, tol=args.tol,
+                                     t_phys=args.t_phys)
+    insts = [b[0] for b in batch]
+    ns = np.array([m["n"] for _, m in batch], dtype=np.int64)
+    S = max(1, args.steps_per_launch)
+    K = (args.steps + S - 1) // S * S
+    W = max(3, (args.warmup + S - 1) // S * S)
+    stream = torch.cuda.current_stream(dev)
+
+    eng = BatchedEngine(_lib.PREC_F32)
+    slots = [eng.add(x) for x in insts]
+    pre = (args.pre_steps // S) * S
+    tune = None
+    if not args.no_tune:
+        from pyheartsim_b200 import autotune
+        tune = autotune.tune(eng, steps=S, stream=stream)
+        pre = max(0, pre - S * 2 * len(tune.get("table", [])))
+    for _ in range(pre // S):
+        eng.advance(S, stream=stream, sync=False)
+    # team sizes from each instance's cost over the warm-up window: the first
+    # rebalance starts the window, the second applies it; the last warm-up
+    # launches capture the CUDA graph of the new plan
+    eng.set_profile(True)
+    for _ in range(3):
+        eng.rebalance()
+        for _ in range(max(1, (W // 4) // S)):
+            eng.advance(S, stream=stream, sync=False)
+    eng.rebalance()
+    eng.set_profile(False)
+    for _ in range(max(1, (W // 4) // S)):
+        eng.advance(S, stream=stream, sync=False)
+    torch.cuda.synchronize(dev)
+    info0 = [eng.info(s) for s in slots]
+    launches0 = eng.launches()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(K // S):
+        eng.advance(S, stream=stream, sync=False)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    launches = eng.launches() - launches0
+    info1 = [eng.info(s) for s in slots]
+    for a, b in zip(info0, info1):
+        assert b["step"] - a["step"] == K, "an instance finished inside the timed window"
+        assert b["status"] in (0, _lib.PHS_WARN_NO_CONVERGE), f"instance status {b['status']}"
+    k_sum = np.array([b["arnoldi_steps"] - a["arnoldi_steps"] for a, b in zip(info0, info1)], dtype=np.float64)
+    k_sq = np.array([b["arnoldi_sq"] - a["arnoldi_sq"] for a, b in zip(info0, info1)], dtype=np.float64)
+    solves = np.array([b["solves"] - a["solves"] for a, b in zip(info0, info1)], dtype=np.float64)
+    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq) for n, ks, kq in zip(ns, k_sum, k_sq)))
+    local_vs = float(ns.sum()) * K
+    total_vs = local_vs * world
+    value = total_vs / (ms_max / 1e3)
+    pk, pk_src = peaks()
+    achieved = alg_bytes / launches / (ms / launches / 1e3) / 1e9 if launches else 0.0
+    phases = phase_profile(eng, slots, S, stream)
+    eng.close()
+
+    line = {"metric": METRIC, "value": value, "unit": "voxel-steps/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded shells; no patient meshes)",
+            "config": {"workload": WORKLOAD, "instances": int(len(ns)), "voxels": int(ns.sum()),
+                       "steps_per_launch": S, "pre_steps": pre, "gmres": f"early exit, tol {args.tol}, restart 20",
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"instance-parallel x{world}"},
+            "gpu_launches": int(launches),
+            "autotune": None if tune is None else {"variant": tune["best"][0], "ctas_per_sm": tune["best"][1],
+                                                   "table": tune.get("table")},
+            "solver": {"arnoldi_per_solve": float(k_sum.sum() / max(solves.sum(), 1)),
+                       "solves_per_step": float(solves.sum() / (K * len(ns))),
+                       "arnoldi_per_step": float(k_sum.sum() / (K * len(ns)))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+                         "traffic": None, "kernel": "step_kernel<float,4>",
+                         "bytes_per_voxel_step": alg_bytes / local_vs},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "phases_ms_per_step": phases}
+
+    if not args.no_extras:
+        line["e2e"] = e2e_leg(args, insts, ns, pre + K, dev)
+        if rank == 0 and world == 1:
+            line["plain_fp64"] = plain_leg(args, batch, value, dev)
+            line["accuracy"] = accuracy_leg(dev, args.tol)
+            line["cpu_baseline"] = cpu_leg(args)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def phase_profile(eng, slots, S, stream):
+    """Device phase timers (first CTA of each team) over 2*S extra steps after the
+    timed region, averaged over instances: ms per step spent in each phase."""
+    import torch
+    eng.set_profile(True)
+    eng.advance(2 * S, stream=stream, sync=True)
+    torch.cuda.synchronize()
+    acc = {}
+    totals = []
+    per = []
+    for s in slots:
+        p = eng.profile(s)
+        st = max(p.pop("steps"), 1)
+        it = p.pop("arnoldi_iters")
+        team = p.pop("team_ctas")
+        inst = eng.instance(s)
+        per.append([int(inst.n_voxel), int(inst.model), int(team), round(it / st, 2),
+                    round(sum(p.values()) / st, 4), round(p["rhs"] / st, 4)])
+        for k, v in p.items():
+            acc[k] = acc.get(k, 0.0) + v / st
+        acc["arnoldi_iters_per_step"] = acc.get("arnoldi_iters_per_step", 0.0) + it / st
+        totals.append(sum(p.values()) / st)
+    eng.set_profile(False)
+    out = {k: round(v / len(slots), 5) for k, v in acc.items()}
+    out["team_ms_per_step_min"] = round(min(totals), 5)
+    out["team_ms_per_step_max"] = round(max(totals), 5)
+    out["per_instance"] = sorted(per, key=lambda r: -r[4])[:12]
+    return out
+
+
+def e2e_leg(args, insts, ns, steps, dev):
+    """The drop-in path with host buffers: upload every instance, run ``steps``
+    steps, download the 1 kHz Vm history and the final state."""
+    import torch
+    from pyheartsim_b200 import _lib
+    from pyheartsim_b200.engine import BatchedEngine
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    eng = BatchedEngine(_lib.PREC_F32)
+    slots = [eng.add(x) for x in insts]
+    h2d = sum(x.nb6.nbytes + x.coef6.nbytes + x.vflags.nbytes + x.stim.nbytes for x in insts)
+    S = max(1, args.steps_per_launch)
+    done = 0
+    while done < steps:
+        k = min(S * 10, steps - done)
+        eng.advance(k, sync=True)
+        done += k
+    d2h = 0
+    for s in slots:
+        hist = eng.history(s)
+        u, h, lat = eng.state(s)
+        d2h += hist.nbytes + u.nbytes + h.nbytes + lat.nbytes
+    t1 = time.perf_counter()
+    eng.close()
+    v = float(ns.sum()) * steps / (t1 - t0)
+    return {"value": v, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "steps": int(steps), "seconds": t1 - t0}
+
+
+def plain_leg(args, batch, fast_value, dev):
+    """Plain FP64 drop-in semantics (full GMRES(50) cycles, FP64) on the median
+    instance, same simulated window as the timed batch."""
+    import torch
+    from pyheartsim_b200 import _lib, workloads
+    from pyheartsim_b200.engine import BatchedEngine
+    ns = np.array([m["n"] for _, m in batch])
+    i = int(np.argsort(ns)[len(ns) // 2])
+    meta = batch[i][1]
+    sizes = workloads.batch_sizes(args.instances, args.n_min, args.n_max, args.seed)
+    inst, _, _ = workloads.shell_case(i, int(sizes[i]), args.seed, fast=False)
+    eng = BatchedEngine(_lib.PREC_F64)
+    slot = eng.add(inst)
+    stream = torch.cuda.current_stream(dev)
+    pre = min(args.pre_steps, 400)
+    eng.advance(pre, stream=stream, sync=True)
+    steps = 20
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    eng.advance(steps, stream=stream, sync=False)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    info = eng.info(slot)
+    eng.close()
+    v = meta["n"] * steps / (ms / 1e3)
+    return {"value": v, "unit": "voxel-steps/s", "instance": i, "voxels": int(meta["n"]), "steps": steps,
+            "arnoldi_per_solve": info["arnoldi_steps"] / max(info["solves"], 1),
+            "speedup_batched_fp32": fast_value / v}
+
+
+def accuracy_leg(dev, tol):
+    """Fast FP32 engine vs the plain FP64 path on a small scarred shell over a
+    whole activation: LAT error in units of dt and max |dVm|."""
+    from pyheartsim_b200.simulation import simulation_gpu
+    from tests import gpu_cases
+    (n, P, geom, sp, ap), pdur = gpu_cases.small_shell_ms(t_phys=60.0)
+    u64, _, _, lat64 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur, return_lat=True)
+    u32, _, _, lat32 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur,
+                                              dtype=np.float32, fast=True, tol=tol, return_lat=True)
+    both = (lat64 >= 0) & (lat32 >= 0)
+    return {"lat_err_max_dt": int(np.abs(lat64[both].astype(np.int64) - lat32[both]).max()) if both.any() else None,
+            "activated_same": bool(np.array_equal(lat64 >= 0, lat32 >= 0)),
+            "max_abs_dvm": float(np.abs(u64 - u32).max()), "voxels": int(n), "ms": 60.0, "tol": tol}
+
+
+def cpu_leg(args):
+    """Port of the reference's legacy CPU stepper on the median MS instance,
+    bounded to ``--cpu-seconds`` of stepping after JIT warm-up."""
+    from oracle import legacy_cpu
+    from pyheartsim_b200 import workloads
+    sizes = workloads.batch_sizes(args.instances, args.n_min, args.n_max, args.seed)
+    i = int(np.argsort(sizes[0::2])[len(sizes[0::2]) // 2]) * 2
+    _, ref_args, meta = workloads.shell_case(i, int(sizes[i]), args.seed)
+    run = legacy_cpu.LegacyRun(*ref_args, pacing_duration=meta["pacing_ms"])
+    for _ in range(3):
+        run.step()
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < args.cpu_seconds:
+        run.step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": meta["n"] * steps / dt, "unit": "voxel-steps/s", "cores": legacy_cpu.threads(), "kind": "port",
+            "sample": f"{steps} steps of instance {i} ({meta['n']} voxels, MS) from t=0 in {dt:.1f} s"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

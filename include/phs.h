@@ -99,6 +99,7 @@ typedef struct phs_instance_info {
     int64_t solves;           /* CN solves that iterated                           */
     int32_t max_arnoldi;      /* most Arnoldi iterations in one solve              */
     int32_t nonconverged;     /* solves that stopped on maxiter                    */
+    int64_t arnoldi_sq;       /* sum over solves of (Arnoldi iterations)^2         */
 } phs_instance_info;
 
 /* ------------------------------------------------ batched engine
@@ -127,6 +128,28 @@ int phs_instance_read_state(phs_engine* eng, int slot, void* u_dst, void* h_dst,
 int phs_instance_device_ptrs(phs_engine* eng, int slot, void** u, void** hist_u, int32_t** lat);
 /* Number of kernel launches the engine issued since creation. */
 int64_t phs_engine_launch_count(phs_engine* eng);
+/* Engine settings.  PHS_CFG_VARIANT: step-kernel variant index (-1 = default);
+ * PHS_CFG_CTAS_PER_SM: CTAs per SM used when advance() is given 0 (0 = occupancy
+ * limit).  Used by the autotuner.                                               */
+#define PHS_CFG_VARIANT      1
+#define PHS_CFG_CTAS_PER_SM  2
+#define PHS_CFG_PROFILE      3   /* 1: per-instance device phase timers on (small overhead) */
+int phs_engine_config(phs_engine* eng, int key, int64_t value);
+/* Compiled step-kernel variants of a precision: count, and per variant the
+ * minimum CTAs per SM it was compiled for and its register count (arrays of at
+ * least *count entries, may be NULL).                                           */
+int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, int32_t* max_regs);
+/* Re-split the CTAs over the instances in proportion to their cost since the
+ * last rebalance: the measured team time per step x team CTAs when the phase
+ * timers (PHS_CFG_PROFILE) are on, else voxels x (1.6 + Arnoldi iterations per
+ * step).  Synchronises the device; the next advance() rebuilds its plan.        */
+int phs_engine_rebalance(phs_engine* eng);
+/* Phase timers of an instance (PHS_CFG_PROFILE on): 16 counters, nanoseconds
+ * spent by the team's first CTA in [0] RHS, [1] its barrier, [2] Arnoldi phase A,
+ * [3] its barrier, [4] phase C, [5] its barrier, [6] update, [7] residual check,
+ * [8] its barrier, [9] final copy, [10] end-of-step barrier; [11] steps and
+ * [12] Arnoldi iterations counted; [13] CTAs in the team at the last launch.   */
+int phs_instance_profile(phs_engine* eng, int slot, uint64_t* out16);
 
 /* ------------------------------------------- one-shot drop-in (host buffers)
  * Runs a whole instance: upload, all steps, download.  Replaces

@@ -29,6 +29,12 @@ PREC_F64 = 64
 EGM_F64 = 0
 EGM_BF16X3 = 1
 
+CFG_VARIANT = 1
+CFG_CTAS_PER_SM = 2
+CFG_PROFILE = 3
+PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
+                 "check", "check_wait", "copy", "step_wait", "steps", "arnoldi_iters", "team_ctas")
+
 VFLAG_S1 = 1
 VFLAG_S2 = 2
 VFLAG_TBLOCK = 4
@@ -82,6 +88,7 @@ class InstanceInfo(ctypes.Structure):
         ("solves", ctypes.c_int64),
         ("max_arnoldi", ctypes.c_int32),
         ("nonconverged", ctypes.c_int32),
+        ("arnoldi_sq", ctypes.c_int64),
     ]
 
 
@@ -104,6 +111,10 @@ SIGNATURES = {
     "phs_instance_device_ptrs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                                 ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(c_int32_p)]),
     "phs_engine_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "phs_engine_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64]),
+    "phs_step_variants": (ctypes.c_int, [ctypes.c_int, c_int32_p, c_int32_p, c_int32_p]),
+    "phs_instance_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
+    "phs_engine_rebalance": (ctypes.c_int, [ctypes.c_void_p]),
     "phs_simulate": (ctypes.c_int, [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                     c_int32_p, c_int32_p, ctypes.POINTER(InstanceInfo)]),
     "phs_egm_leadfield_f64": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,

@@ -60,6 +60,12 @@ enum Action : int {
 
 enum Phase : int { PH_PLAIN = 0, PH_RHS = 1, PH_DOTS = 2, PH_NORM = 3, PH_CHECK = 4 };
 
+// Phase timer slots (nanoseconds of globaltimer, summed over steps).
+enum ProfSlot : int {
+    PF_RHS = 0, PF_RHS_WAIT, PF_A, PF_A_WAIT, PF_C, PF_C_WAIT, PF_X, PF_CHECK, PF_CHECK_WAIT,
+    PF_COPY, PF_STEP_WAIT, PF_STEPS, PF_SOLVE_ITERS, PF_TEAM, kProfSlots = 16
+};
+
 struct Scalars {
     double R[(kMaxRestart + 1) * kMaxRestart];  // column j at R[j*(kMaxRestart+1) + i]
     double cs[kMaxRestart];
@@ -84,6 +90,7 @@ struct InstState {
     long long solves;
     int max_arnoldi;
     int nonconv;
+    long long arnoldi_sq;  // sum over solves of (Arnoldi steps)^2
 };
 
 template <typename T>
@@ -106,6 +113,7 @@ struct InstDev {
     Scalars* sc;
     TeamSync* sync;
     InstState* st;
+    unsigned long long* prof;  // [kProfSlots] phase timers (CTA rank 0 of the team), or nullptr
     T params[5];
     T dt, half_dt, jmag;
     double tol, atol;
@@ -113,6 +121,7 @@ struct InstDev {
     long long n_steps;
     long long tb_steps;
     int n_tiles;
+    int ps;                 // partial slots per (tile, warp): m + 2
     int model;
     int m;                  // restart length actually used: min(restart, n)
     int maxiter;
@@ -136,22 +145,59 @@ __device__ __forceinline__ void reaction(int model, T u, T h, T J, const T* p, T
     }
 }
 
+// FP32 form of the same right-hand sides: the Mitchell-Schaeffer time
+// constants enter as precomputed reciprocals (q[0] = 1/tau_open, q[1] =
+// 1/tau_close, q[2] = 1/tau_in, q[3] = 1/tau_out, q[4] = v_gate) and the
+// Aliev-Panfilov quotient uses the fast division; FP64 keeps the reference's
+// divisions exactly.
+__device__ __forceinline__ void reaction_fast(int model, float u, float h, float J, const float* q, float& du,
+                                              float& dh) {
+    if (model == 0) {
+        du = h * (u * u) * (1.0f - u) * q[2] - u * q[3] + J;
+        dh = (u < q[4]) ? (1.0f - h) * q[0] : -h * q[1];
+    } else {
+        du = -q[0] * u * (u - q[1]) * (u - 1.0f) - u * h + J;
+        dh = (q[2] + q[3] * __fdividef(h, u + q[4])) * (-h - q[0] * u * (u - q[1] - 1.0f));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void reaction_any(int model, T u, T h, T J, const T* p, T& du, T& dh) {
+    if constexpr (sizeof(T) == 4) reaction_fast(model, u, h, J, p, du, dh);
+    else reaction(model, u, h, J, p, du, dh);
+}
+
 // Classical RK4 with J held over the step, simulation/simulation_gpu.py:71-130.
+// `p` holds P_2d columns 15..19 (FP64) or their FP32 form (see reaction_fast).
 template <typename T>
 __device__ __forceinline__ void rk4(int model, T u, T h, T J, const T* p, T dt, T& us, T& hs) {
     T k1u, k1h, k2u, k2h, k3u, k3h, k4u, k4h;
-    reaction(model, u, h, J, p, k1u, k1h);
+    reaction_any(model, u, h, J, p, k1u, k1h);
     T ut = u + T(0.5) * dt * k1u;
     T ht = h + T(0.5) * dt * k1h;
-    reaction(model, ut, ht, J, p, k2u, k2h);
+    reaction_any(model, ut, ht, J, p, k2u, k2h);
     ut = u + T(0.5) * dt * k2u;
     ht = h + T(0.5) * dt * k2h;
-    reaction(model, ut, ht, J, p, k3u, k3h);
+    reaction_any(model, ut, ht, J, p, k3u, k3h);
     ut = u + dt * k3u;
     ht = h + dt * k3h;
-    reaction(model, ut, ht, J, p, k4u, k4h);
+    reaction_any(model, ut, ht, J, p, k4u, k4h);
     us = u + (dt / T(6)) * (k1u + T(2) * k2u + T(2) * k3u + k4u);
     hs = h + (dt / T(6)) * (k1h + T(2) * k2h + T(2) * k3h + k4h);
+}
+
+// P_2d columns 15..19 -> the parameter form rk4<T> expects.
+template <typename T>
+__host__ __device__ __forceinline__ void model_form(int model, const T* p, T* q) {
+    if (sizeof(T) == 4 && model == 0) {
+        q[0] = T(1) / p[0];
+        q[1] = T(1) / p[1];
+        q[2] = T(1) / p[2];
+        q[3] = T(1) / p[3];
+        q[4] = p[4];
+    } else {
+        for (int i = 0; i < 5; ++i) q[i] = p[i];
+    }
 }
 
 // ------------------------------------------------------------------ helpers
@@ -230,18 +276,60 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
     return ctl.abort == 0;
 }
 
-// Leader helper: sum slot `slot` over all tiles in tile order (deterministic).
-// Called by one warp; returns the sum in every lane.
-__device__ __forceinline__ double tile_sum(const double* part, int n_tiles, int slot) {
+// Leader helper: sum one partial slot over every (tile, warp) of the instance in
+// (tile, warp) order.  Lane l sums entries l, l+32, ... and the lanes combine in
+// a fixed xor tree, so the result does not depend on which CTA processed which
+// tile.  Called by one warp; returns the sum in every lane.
+__device__ __forceinline__ double tile_sum(const double* part, int count, int ps, int slot) {
     const int lane = threadIdx.x & 31;
-    double acc = 0.0;
-    for (int t = lane; t < n_tiles; t += 32) acc += __ldcg(part + (size_t)t * kSlots + slot);
-    return warp_sum(acc);
+    double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int q = lane;
+    for (; q + 7 * 32 < count; q += 8 * 32) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a[u] += __ldcg(part + (size_t)(q + 32 * u) * ps + slot);
+    }
+    for (; q < count; q += 32) a[0] += __ldcg(part + (size_t)q * ps + slot);
+    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    return warp_sum(s);
 }
 
+// The six (neighbour, coefficient) pairs of row n, as 8/16-byte vector loads.
+__device__ __forceinline__ void load_nb(const int32_t* nb, long long n, int32_t (&q)[6]) {
+    const int2* p = reinterpret_cast<const int2*>(nb + 6 * n);
+    int2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+    q[0] = a.x; q[1] = a.y; q[2] = b.x; q[3] = b.y; q[4] = c.x; q[5] = c.y;
+}
+__device__ __forceinline__ void load_coef(const float* cf, long long n, float (&c)[6]) {
+    const float2* p = reinterpret_cast<const float2*>(cf + 6 * n);
+    float2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
+    c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y; c[4] = d.x; c[5] = d.y;
+}
+__device__ __forceinline__ void load_coef(const double* cf, long long n, double (&c)[6]) {
+    const double2* p = reinterpret_cast<const double2*>(cf + 6 * n);
+    double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
+    c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y; c[4] = d.x; c[5] = d.y;
+}
+
+// Matrix-free row of L applied to `vec` at voxel n (coefficients already loaded);
+// all six gathers are issued before they are combined.
+template <typename T>
+__device__ __forceinline__ T lap_row(const T* vec, T vn, const int32_t (&q)[6], const T (&c)[6]) {
+    T g[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g[k] = (c[k] != T(0)) ? vec[q[k]] : vn;
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc += c[k] * (g[k] - vn);
+    return acc;
+}
+
+constexpr int kChunk = 4;  // basis vectors whose loads are issued together
+template <typename T>
+constexpr bool kWarpParts = sizeof(T) == 4;
+
 // ------------------------------------------------------------------ the kernel
-template <typename T, int VPT>
-__global__ void __launch_bounds__(kThreads)
+template <typename T, int VPT, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_map,
             long long n_steps_launch, unsigned int* abort_word) {
     constexpr int TILE = kThreads * VPT;
@@ -251,8 +339,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     __shared__ InstDev<T> I;
     __shared__ SharedCtl ctl;
-    __shared__ double red[kWarps][kSlots];
     __shared__ double shc[kMaxRestart + 1];
+    __shared__ T ustar_tile[TILE];
     __shared__ long long sh_step0;
     __shared__ int sh_id_save, sh_pending, sh_hbuf, sh_status;
 
@@ -267,7 +355,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     __syncthreads();
 
     const long long N = I.n;
-    const int m = I.m;
+    const int ps = I.ps;
+    const int nparts = kWarpParts<T> ? I.n_tiles * kWarps : I.n_tiles;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     Scalars* sc = I.sc;
@@ -279,38 +368,55 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     int hbuf = sh_hbuf;
     bool retired = (sh_status == PHS_ERR_NONFINITE);
     bool aborted = false;
-
-    // ---- tile partial writer: threads 0..nslot-1 sum the kWarps warp partials
-    auto write_partials = [&](int tile, int nslot) {
-        __syncthreads();
-        for (int t = threadIdx.x; t < nslot; t += kThreads) {
-            double s = 0.0;
-#pragma unroll
-            for (int w = 0; w < kWarps; ++w) s += red[w][t];
-            I.part[(size_t)tile * kSlots + t] = s;
+    // optional phase timer: thread 0 of CTA rank 0 of each team
+    __shared__ unsigned long long pf[kProfSlots];
+    __shared__ unsigned long long pf_t;
+    const bool prof_on = (I.prof != nullptr) && rank == 0;
+    if (prof_on && threadIdx.x == 0) {
+        for (int i = 0; i < kProfSlots; ++i) pf[i] = 0ull;
+        pf_t = global_ns();
+    }
+    auto mark = [&](int slot) {
+        if (prof_on && threadIdx.x == 0) {
+            unsigned long long t = global_ns();
+            pf[slot] += t - pf_t;
+            pf_t = t;
         }
-        __syncthreads();
     };
 
-    // ---- stencil of a vector at voxel n (matrix-free row of L)
-    auto lap_at = [&](const T* vec, long long n, T vn, bool rowzero) -> T {
-        T acc = T(0);
-        if (!rowzero) {
-            const int32_t* nbp = I.nb + 6 * n;
-            const T* cp = I.coef + 6 * n;
+    // Partial sums of one tile.  FP32: one entry per (tile, warp), written by
+    // lane 0 after a warp reduction.  FP64 (long GMRES(50) cycles): the warps of
+    // a tile are first combined in shared memory, one entry per tile, so the
+    // leader reads 8x fewer values.  Both orders are fixed.
+    __shared__ double red[2][kWarps][kSlots];
+    int red_buf = 0;
+    auto put = [&](int tile, int slot, double v) {
+        if constexpr (kWarpParts<T>) {
+            if (lane == 0) I.part[(size_t)(tile * kWarps + warp) * ps + slot] = v;
+        } else {
+            if (lane == 0) red[red_buf][warp][slot] = v;
+        }
+    };
+    auto tile_done = [&](int tile, int nslot) {
+        if constexpr (!kWarpParts<T>) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < nslot; t += kThreads) {
+                double a = 0.0;
 #pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                T c = cp[k];
-                if (c != T(0)) acc += c * (vec[nbp[k]] - vn);
+                for (int w = 0; w < kWarps; ++w) a += red[red_buf][w][t];
+                I.part[(size_t)tile * ps + t] = a;
             }
+            red_buf ^= 1;
         }
-        return acc;
     };
+    auto voxel = [&](int tile, int v) -> long long { return (long long)tile * TILE + v * kThreads + threadIdx.x; };
 
     auto params_of = [&](long long n, T* p) {
         if (I.vparams) {
+            T raw[5];
 #pragma unroll
-            for (int q = 0; q < 5; ++q) p[q] = I.vparams[5 * n + q];
+            for (int q = 0; q < 5; ++q) raw[q] = I.vparams[5 * n + q];
+            model_form<T>(I.model, raw, p);
         } else {
 #pragma unroll
             for (int q = 0; q < 5; ++q) p[q] = I.params[q];
@@ -319,9 +425,15 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     // ---- leader bodies ------------------------------------------------------
     auto leader_rhs = [&]() {
+        __shared__ double s_r2;
+        if (warp == 1) {
+            double r2 = tile_sum(I.part, nparts, ps, 1);
+            if (lane == 0) s_r2 = r2;
+        }
+        __syncthreads();
         if (warp == 0) {
-            double b2 = tile_sum(I.part, I.n_tiles, 0);
-            double r2 = tile_sum(I.part, I.n_tiles, 1);
+            double b2 = tile_sum(I.part, nparts, ps, 0);
+            double r2 = s_r2;
             if (lane == 0) {
                 double bn = sqrt(b2), rn = sqrt(r2);
                 double atol_eff = fmax(I.atol, I.tol * bn);
@@ -346,9 +458,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     auto leader_dots = [&](int j) {
-        // h_ij = s_i * sum_tiles <V_i, w>;  published coef_i = h_ij * s_i
+        // h_ij = s_i * sum <V_i, w>;  published coef_i = h_ij * s_i
         for (int i = warp; i <= j; i += kWarps) {
-            double d = tile_sum(I.part, I.n_tiles, i);
+            double d = tile_sum(I.part, nparts, ps, i);
             if (lane == 0) {
                 double si = sc->s[i];
                 double h = si * d;
@@ -360,7 +472,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     auto leader_norm = [&](int j) {
         if (warp == 0) {
-            double u2 = tile_sum(I.part, I.n_tiles, 0);
+            double u2 = tile_sum(I.part, nparts, ps, 0);
             if (lane == 0) {
                 double* Rc = sc->R + j * (kMaxRestart + 1);
                 double hn = sqrt(u2);
@@ -428,7 +540,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     auto leader_check = [&]() {
         if (warp == 0) {
-            double r2 = tile_sum(I.part, I.n_tiles, 0);
+            double r2 = tile_sum(I.part, nparts, ps, 0);
             if (lane == 0) {
                 double rn = sqrt(r2);
                 sc->rnorm = rn;
@@ -458,6 +570,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             int it = sc->iters_solve;
             if (it > 0) {
                 I.st->arnoldi += it;
+                I.st->arnoldi_sq += (long long)it * it;
                 I.st->solves += 1;
                 if (it > I.st->max_arnoldi) I.st->max_arnoldi = it;
             }
@@ -473,7 +586,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         return ctl.action;
     };
 
-    auto load_coef = [&](int cnt) {
+    auto load_shc = [&](int cnt) {
+        __syncthreads();
         for (int i = threadIdx.x; i < cnt; i += kThreads) shc[i] = __ldcg(sc->coef + i);
         __syncthreads();
     };
@@ -484,56 +598,107 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             I.hist_u[(size_t)pending * N + n] = un;
             if (I.save_h) I.hist_h[(size_t)pending * N + n] = hn;
         }
-        if (done_step >= 0 && I.lat[n] < 0 && un >= T(0.5)) I.lat[n] = (int32_t)done_step;
+        if (done_step >= 0 && un >= T(0.5) && I.lat[n] < 0) I.lat[n] = (int32_t)done_step;
     };
 
+    // acc[v] += sum_{i < cnt} coef[i] * Vb[i][n_v], loads issued kChunk vectors at a time
     T* Vb = I.V;
     const size_t ldV = (size_t)N;
+    auto axpy_basis = [&](int tile, int cnt, const double* coef, double (&acc)[VPT]) {
+        for (int i0 = 0; i0 < cnt; i0 += kChunk) {
+            T vv[kChunk][VPT];
+#pragma unroll
+            for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    long long n = voxel(tile, v);
+                    vv[ii][v] = (i0 + ii < cnt && n < N) ? Vb[(size_t)(i0 + ii) * ldV + n] : T(0);
+                }
+#pragma unroll
+            for (int ii = 0; ii < kChunk; ++ii) {
+                if (i0 + ii < cnt) {
+                    const double cf = coef[i0 + ii];
+#pragma unroll
+                    for (int v = 0; v < VPT; ++v) acc[v] += cf * (double)vv[ii][v];
+                }
+            }
+        }
+    };
 
     for (; step < step_end && !retired && !aborted; ++step) {
-        const uint8_t stim_bits = I.stim[step];
+        const uint8_t stim_bits = __ldg(I.stim + step);
         const bool tb = step < I.tb_steps;
         const T* hin = hbuf ? I.h1 : I.h0;
         T* hout = hbuf ? I.h0 : I.h1;
 
-        // ================= RHS phase: fused RK4 + b + r0
+        // ================= RHS phase: fused RK4 + b + r0.  The tile's own u* stay
+        // in shared memory; only neighbours outside the tile are recomputed.
         for (int tile = rank; tile < I.n_tiles; tile += P) {
-            double ab = 0.0, ar = 0.0;
+            const long long base = (long long)tile * TILE;
+            T us_reg[VPT];
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
-                long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                const long long n = voxel(tile, v);
+                us_reg[v] = T(0);
                 if (n < N) {
-                    T un = I.u[n], hn = hin[n];
+                    const T un = I.u[n], hn = hin[n];
+                    const uint8_t f = __ldg(I.vflags + n);
                     sample_voxel(n, un, hn, step - 1);
-                    uint8_t f = I.vflags[n];
                     T p[5];
                     params_of(n, p);
-                    T J = (f & stim_bits & 3u) ? I.jmag : T(0);
+                    const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
                     T us, hs;
                     rk4(I.model, un, hn, J, p, I.dt, us, hs);
                     I.x[n] = us;
                     hout[n] = hs;
+                    us_reg[v] = us;
+                    ustar_tile[v * kThreads + threadIdx.x] = us;
+                }
+            }
+            __syncthreads();
+            double ab = 0.0, ar = 0.0;
+#pragma unroll 1
+            for (int v = 0; v < VPT; ++v) {
+                const long long n = voxel(tile, v);
+                if (n < N) {
+                    const T us = us_reg[v];
+                    const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
+                    int32_t q[6];
+                    T c[6];
+                    load_nb(I.nb, n, q);
+                    load_coef(I.coef, n, c);
                     T lap = T(0);
-                    if (!(tb && (f & PHS_VFLAG_TBLOCK))) {
-                        const int32_t* nbp = I.nb + 6 * n;
-                        const T* cp = I.coef + 6 * n;
+                    if (!rz) {
+                        T uq[6], hq[6];
+                        uint8_t fq[6];
+                        bool far[6];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) {
+                            const long long off = (long long)q[k] - base;
+                            far[k] = (c[k] != T(0)) && (off < 0 || off >= TILE);
+                            uq[k] = far[k] ? I.u[q[k]] : T(0);
+                            hq[k] = far[k] ? hin[q[k]] : T(0);
+                            fq[k] = far[k] ? __ldg(I.vflags + q[k]) : (uint8_t)0;
+                        }
 #pragma unroll 1
                         for (int k = 0; k < 6; ++k) {
-                            T c = cp[k];
-                            if (c != T(0)) {
-                                int32_t q = nbp[k];
+                            if (c[k] == T(0)) continue;
+                            T usq;
+                            if (far[k]) {
                                 T pq[5];
-                                params_of(q, pq);
-                                T Jq = (I.vflags[q] & stim_bits & 3u) ? I.jmag : T(0);
-                                T usq, hsq;
-                                rk4(I.model, I.u[q], hin[q], Jq, pq, I.dt, usq, hsq);
-                                lap += c * (usq - us);
+                                params_of(q[k], pq);
+                                const T Jq = (fq[k] & stim_bits & 3u) ? I.jmag : T(0);
+                                T hsq;
+                                rk4(I.model, uq[k], hq[k], Jq, pq, I.dt, usq, hsq);
+                            } else {
+                                usq = ustar_tile[q[k] - base];
                             }
+                            lap += c[k] * (usq - us);
                         }
                     }
-                    T bn = us + I.half_dt * lap;
-                    T ax = us - I.half_dt * lap;
-                    T rn = bn - ax;
+                    const T bn = us + I.half_dt * lap;
+                    const T ax = us - I.half_dt * lap;
+                    const T rn = bn - ax;
                     I.b[n] = bn;
                     Vb[n] = rn;
                     ab += (double)bn * (double)bn;
@@ -542,12 +707,16 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             }
             ab = warp_sum(ab);
             ar = warp_sum(ar);
-            if (lane == 0) { red[warp][0] = ab; red[warp][1] = ar; }
-            write_partials(tile, 2);
+            put(tile, 0, ab);
+            put(tile, 1, ar);
+            tile_done(tile, 2);
+            __syncthreads();   // ustar_tile is rewritten by the next tile
         }
         pending = -1;
+        mark(PF_RHS);
         if (!team_sync(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
         int act = read_action();
+        mark(PF_RHS_WAIT);
 
         if (act == ACT_CYCLE) {
             bool leave_solve = false;
@@ -564,52 +733,91 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                         T wr[VPT];
 #pragma unroll
                         for (int v = 0; v < VPT; ++v) {
-                            long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                            const long long n = voxel(tile, v);
                             wr[v] = T(0);
                             if (n < N) {
-                                T vj = Vj[n];
-                                bool rz = tb && (I.vflags[n] & PHS_VFLAG_TBLOCK);
-                                T lap = lap_at(Vj, n, vj, rz);
-                                T w = sj * (vj - I.half_dt * lap);
+                                const T vj = Vj[n];
+                                const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
+                                int32_t q[6];
+                                T c[6];
+                                load_nb(I.nb, n, q);
+                                load_coef(I.coef, n, c);
+                                const T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
+                                const T w = sj * (vj - I.half_dt * lap);
                                 Vn[n] = w;
                                 wr[v] = w;
                             }
                         }
-                        for (int i = 0; i <= j; ++i) {
-                            const T* Vi = Vb + (size_t)i * ldV;
-                            double d = 0.0;
+                        for (int i0 = 0; i0 <= j; i0 += kChunk) {
+                            T vv[kChunk][VPT];
 #pragma unroll
-                            for (int v = 0; v < VPT; ++v) {
-                                long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
-                                if (n < N) d += (double)Vi[n] * (double)wr[v];
+                            for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                                for (int v = 0; v < VPT; ++v) {
+                                    const long long n = voxel(tile, v);
+                                    vv[ii][v] = (i0 + ii <= j && n < N) ? Vb[(size_t)(i0 + ii) * ldV + n] : T(0);
+                                }
+#pragma unroll
+                            for (int ii = 0; ii < kChunk; ++ii) {
+                                double d = 0.0;
+#pragma unroll
+                                for (int v = 0; v < VPT; ++v) d += (double)vv[ii][v] * (double)wr[v];
+                                d = warp_sum(d);
+                                if (i0 + ii <= j) put(tile, i0 + ii, d);
                             }
-                            d = warp_sum(d);
-                            if (lane == 0) red[warp][i] = d;
                         }
-                        write_partials(tile, j + 1);
+                        tile_done(tile, j + 1);
                     }
+                    mark(PF_A);
                     if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_dots(j); })) { aborted = true; break; }
-                    load_coef(j + 1);
+                    load_shc(j + 1);
+                    mark(PF_A_WAIT);
                     // ============ phase C: u = w - sum_i c_i V_i  (in place), ||u||^2
                     for (int tile = rank; tile < I.n_tiles; tile += P) {
+                        double acc[VPT];
+#pragma unroll
+                        for (int v = 0; v < VPT; ++v) {
+                            const long long n = voxel(tile, v);
+                            acc[v] = (n < N) ? (double)Vn[n] : 0.0;
+                        }
+                        // acc -= sum_i shc[i] V_i
+                        for (int i0 = 0; i0 <= j; i0 += kChunk) {
+                            T vv[kChunk][VPT];
+#pragma unroll
+                            for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                                for (int v = 0; v < VPT; ++v) {
+                                    const long long n = voxel(tile, v);
+                                    vv[ii][v] = (i0 + ii <= j && n < N) ? Vb[(size_t)(i0 + ii) * ldV + n] : T(0);
+                                }
+#pragma unroll
+                            for (int ii = 0; ii < kChunk; ++ii) {
+                                if (i0 + ii <= j) {
+                                    const double cf = shc[i0 + ii];
+#pragma unroll
+                                    for (int v = 0; v < VPT; ++v) acc[v] -= cf * (double)vv[ii][v];
+                                }
+                            }
+                        }
                         double a2 = 0.0;
 #pragma unroll
                         for (int v = 0; v < VPT; ++v) {
-                            long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                            const long long n = voxel(tile, v);
                             if (n < N) {
-                                double uu = (double)Vn[n];
-                                for (int i = 0; i <= j; ++i) uu -= shc[i] * (double)Vb[(size_t)i * ldV + n];
-                                T ut = (T)uu;
+                                const T ut = (T)acc[v];
                                 Vn[n] = ut;
                                 a2 += (double)ut * (double)ut;
                             }
                         }
                         a2 = warp_sum(a2);
-                        if (lane == 0) red[warp][0] = a2;
-                        write_partials(tile, 1);
+                        put(tile, 0, a2);
+                        tile_done(tile, 1);
                     }
+                    mark(PF_C);
                     if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_norm(j); })) { aborted = true; break; }
                     act = read_action();
+                    mark(PF_C_WAIT);
+                    if (prof_on && threadIdx.x == 0) pf[PF_SOLVE_ITERS] += 1;
                     if (act != ACT_NEXT_J) break;
                     ++j;
                 }
@@ -617,20 +825,26 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 if (act == ACT_FAIL) { retired = true; break; }
                 // ============ phase X: x += sum_j c_j V_j
                 const int k = ctl.k;
-                load_coef(k);
+                load_shc(k);
                 const bool final = (act == ACT_UPDATE_FINAL);
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
+                    double acc[VPT];
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
-                        long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                        const long long n = voxel(tile, v);
+                        acc[v] = (n < N) ? (double)I.x[n] : 0.0;
+                    }
+                    axpy_basis(tile, k, shc, acc);
+#pragma unroll
+                    for (int v = 0; v < VPT; ++v) {
+                        const long long n = voxel(tile, v);
                         if (n < N) {
-                            double xv = (double)I.x[n];
-                            for (int jj = 0; jj < k; ++jj) xv += shc[jj] * (double)Vb[(size_t)jj * ldV + n];
-                            if (final) I.u[n] = (T)xv;
-                            else I.x[n] = (T)xv;
+                            if (final) I.u[n] = (T)acc[v];
+                            else I.x[n] = (T)acc[v];
                         }
                     }
                 }
+                mark(PF_X);
                 if (final) break;
                 // ============ true residual of the new iterate (start of the next cycle)
                 if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
@@ -638,24 +852,30 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     double a2 = 0.0;
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
-                        long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                        const long long n = voxel(tile, v);
                         if (n < N) {
-                            T xv = I.x[n];
-                            bool rz = tb && (I.vflags[n] & PHS_VFLAG_TBLOCK);
-                            T lap = lap_at(I.x, n, xv, rz);
-                            T ax = xv - I.half_dt * lap;
-                            T r = I.b[n] - ax;
+                            const T xv = I.x[n];
+                            const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
+                            int32_t q[6];
+                            T c[6];
+                            load_nb(I.nb, n, q);
+                            load_coef(I.coef, n, c);
+                            const T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
+                            const T ax = xv - I.half_dt * lap;
+                            const T r = I.b[n] - ax;
                             Vb[n] = r;
                             I.u[n] = xv;
                             a2 += (double)r * (double)r;
                         }
                     }
                     a2 = warp_sum(a2);
-                    if (lane == 0) red[warp][0] = a2;
-                    write_partials(tile, 1);
+                    put(tile, 0, a2);
+                    tile_done(tile, 1);
                 }
+                mark(PF_CHECK);
                 if (!team_sync(I.sync, P, abort_word, ctl, leader_check)) { aborted = true; break; }
                 act = read_action();
+                mark(PF_CHECK_WAIT);
                 if (act == ACT_DONE) break;
                 if (act == ACT_FAIL) { retired = true; break; }
                 // ACT_CYCLE: V0 holds the new residual
@@ -666,7 +886,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             for (int tile = rank; tile < I.n_tiles; tile += P) {
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
-                    long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                    const long long n = voxel(tile, v);
                     if (n < N) I.u[n] = src[n];
                 }
             }
@@ -674,8 +894,11 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             retired = true;
             break;
         }
+        mark(PF_COPY);
         // end of step: u visible to every CTA of the team; solve statistics
         if (!team_sync(I.sync, P, abort_word, ctl, leader_solve_stats)) { aborted = true; break; }
+        mark(PF_STEP_WAIT);
+        if (prof_on && threadIdx.x == 0) pf[PF_STEPS] += 1;
         hbuf ^= 1;
         const bool due = (I.stride > 0) ? (step % I.stride == 0) : true;
         if (due && id_save < I.n_samples) pending = id_save++;
@@ -688,12 +911,16 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             for (int tile = rank; tile < I.n_tiles; tile += P) {
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
-                    long long n = (long long)tile * TILE + v * kThreads + threadIdx.x;
+                    const long long n = voxel(tile, v);
                     if (n < N) sample_voxel(n, I.u[n], hcur[n], step - 1);
                 }
             }
         }
         pending = -1;
+    }
+    if (prof_on && threadIdx.x == 0) {
+        for (int i = 0; i < PF_TEAM; ++i) atomicAdd(I.prof + i, pf[i]);
+        atomicExch(I.prof + PF_TEAM, (unsigned long long)P);
     }
     if (!aborted) {
         if (!team_sync(I.sync, P, abort_word, ctl, [&]() {
@@ -734,6 +961,24 @@ namespace {
 constexpr int kVptF32 = 4;
 constexpr int kVptF64 = 1;
 
+// Compiled step-kernel variants: same algorithm and tiling, different register
+// budgets (__launch_bounds__ minimum CTAs per SM).  The autotuner picks one.
+using StepFnF = void (*)(const InstDev<float>*, const int4*, long long, unsigned int*);
+using StepFnD = void (*)(const InstDev<double>*, const int4*, long long, unsigned int*);
+const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2>, step_kernel<float, kVptF32, 3>,
+                            step_kernel<float, kVptF32, 4>};
+const int kMinbF32[] = {2, 3, 4};
+const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2>, step_kernel<double, kVptF64, 3>};
+const int kMinbF64[] = {2, 3};
+constexpr int kNumF32 = 3, kNumF64 = 2;
+constexpr int kDefaultF32 = 1, kDefaultF64 = 0;
+
+template <typename T>
+const void* step_fn(int variant) {
+    if (sizeof(T) == 8) return (const void*)kStepF64[variant];
+    return (const void*)kStepF32[variant];
+}
+
 struct InstHost {
     bool used = false;
     bool finished = false;
@@ -759,12 +1004,19 @@ struct InstHost {
     Scalars* sc = nullptr;
     TeamSync* sync = nullptr;
     InstState* st = nullptr;
+    unsigned long long* prof = nullptr;
     InstState st_host{};
+    double kavg = 4.0;           // recent Arnoldi steps per step (cost model)
+    long long ref_arnoldi = 0;   // counters at the last rebalance
+    long long ref_step = 0;
+    double weight = 0.0;         // measured CTA-time per step (0: use the model)
+    int team = 0;                // CTAs given to this instance by the current plan
+    unsigned long long prof_ref[16] = {};
 };
 
 void free_inst(InstHost& h) {
     void* ptrs[] = {h.nb, h.coef, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
-                    h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st};
+                    h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     h = InstHost();
@@ -784,18 +1036,24 @@ struct phs_engine {
     size_t d_map_n = 0;
     long long launches = 0;
     bool broken = false;
+    // cached launch plan (rebuilt when the instance set changes)
+    bool dirty = true;
+    std::vector<int> act;
+    std::vector<std::pair<size_t, int>> waves;
+    int plan_cps = -1;
+    // CUDA graphs of the launch sequence, keyed by steps per launch
+    std::map<long long, cudaGraphExec_t> graphs;
+    bool graphs_ok = true;
+    int variant = -1;        // step-kernel variant (-1: default of the precision)
+    bool profile = false;    // per-instance phase timers
+    int default_cps = 0;     // CTAs per SM when advance() is given 0 (0: occupancy limit)
 };
 
 namespace {
 
 template <typename T>
-int occupancy_for(int* ctas) {
-    int vpt = sizeof(T) == 8 ? kVptF64 : kVptF32;
-    cudaError_t e;
-    if (vpt == 1)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_kernel<T, 1>, kThreads, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_kernel<T, kVptF32>, kThreads, 0);
+int occupancy_for(int* ctas, int variant) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_fn<T>(variant), kThreads, 0);
     if (e != cudaSuccess) { set_last_error("occupancy", e); return PHS_ERR_CUDA; }
     return PHS_OK;
 }
@@ -888,7 +1146,8 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     PHS_ALLOC(h.hist_u, S * n * sizeof(T));
     if (d->save_h) PHS_ALLOC(h.hist_h, S * n * sizeof(T));
     PHS_ALLOC(h.lat, n * sizeof(int32_t));
-    PHS_ALLOC(h.part, (size_t)h.n_tiles * kSlots * sizeof(double));
+    const size_t nparts = (size_t)h.n_tiles * (kWarpParts<T> ? kWarps : 1);
+    PHS_ALLOC(h.part, nparts * (h.m + 2) * sizeof(double));
     PHS_ALLOC(h.sc, sizeof(Scalars));
     PHS_ALLOC(h.sync, sizeof(TeamSync));
     PHS_ALLOC(h.st, sizeof(InstState));
@@ -902,7 +1161,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     cudaMemset(h.hist_u, 0, S * n * sizeof(T));
     if (h.hist_h) cudaMemset(h.hist_h, 0, S * n * sizeof(T));
     cudaMemset(h.lat, 0xff, n * sizeof(int32_t));
-    cudaMemset(h.part, 0, (size_t)h.n_tiles * kSlots * sizeof(double));
+    cudaMemset(h.part, 0, nparts * (h.m + 2) * sizeof(double));
     cudaMemset(h.sc, 0, sizeof(Scalars));
     cudaMemset(h.sync, 0, sizeof(TeamSync));
     InstState st{};
@@ -921,7 +1180,12 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     for (size_t i = 0; i < e->inst.size(); ++i)
         if (!e->inst[i].used) { s = (int)i; break; }
     if (s < 0) { s = (int)e->inst.size(); e->inst.push_back(InstHost()); }
+    if (e->profile) {
+        if (cudaMalloc((void**)&h.prof, kProfSlots * sizeof(unsigned long long)) == cudaSuccess)
+            cudaMemset(h.prof, 0, kProfSlots * sizeof(unsigned long long));
+    }
     e->inst[s] = h;
+    e->dirty = true;
     *slot = s;
     return PHS_OK;
 }
@@ -947,7 +1211,10 @@ InstDev<T> make_dev(const InstHost& h) {
     I.sc = h.sc;
     I.sync = h.sync;
     I.st = h.st;
-    for (int q = 0; q < 5; ++q) I.params[q] = (T)h.d.params[q];
+    I.prof = h.prof;
+    T raw[5];
+    for (int q = 0; q < 5; ++q) raw[q] = (T)h.d.params[q];
+    model_form<T>(h.d.model, raw, I.params);
     I.dt = (T)h.d.dt;
     I.half_dt = (T)h.d.dt / T(2);
     I.jmag = (T)h.d.j_stim;
@@ -957,6 +1224,7 @@ InstDev<T> make_dev(const InstHost& h) {
     I.n_steps = h.d.n_steps;
     I.tb_steps = h.d.tblock_steps;
     I.n_tiles = h.n_tiles;
+    I.ps = h.m + 2;
     I.model = h.d.model;
     I.m = h.m;
     I.maxiter = h.d.maxiter;
@@ -967,16 +1235,18 @@ InstDev<T> make_dev(const InstHost& h) {
     return I;
 }
 
-// Split G CTAs over the instances in proportion to their tiles (at least one
-// CTA each, never more CTAs than tiles).
-std::vector<int> team_sizes(const std::vector<int>& tiles, int G) {
+// Split G CTAs over the instances in proportion to their cost (voxels times
+// the cost of a step in units of one Arnoldi iteration: the RHS, update and
+// copy phases weigh about 1.6 iterations), at least one CTA each and never
+// more CTAs than tiles.
+std::vector<int> team_sizes(const std::vector<int>& tiles, const std::vector<double>& weight, int G) {
     const int A = (int)tiles.size();
     std::vector<int> P(A, 1);
-    long long total = 0;
-    for (int t : tiles) total += t;
+    double total = 0.0;
+    for (double w : weight) total += w;
     int used = A;
     for (int i = 0; i < A; ++i) {
-        long long want = (long long)((double)G * tiles[i] / (double)std::max<long long>(total, 1));
+        long long want = (long long)((double)G * weight[i] / std::max(total, 1e-30));
         int p = (int)std::max<long long>(1, std::min<long long>(want, tiles[i]));
         used += p - 1;
         P[i] = p;
@@ -986,7 +1256,7 @@ std::vector<int> team_sizes(const std::vector<int>& tiles, int G) {
         double best_ratio = 0.0;
         for (int i = 0; i < A; ++i) {
             if (P[i] >= tiles[i]) continue;
-            double r = (double)tiles[i] / P[i];
+            double r = weight[i] / P[i];
             if (r > best_ratio) { best_ratio = r; best = i; }
         }
         if (best < 0) break;
@@ -998,7 +1268,7 @@ std::vector<int> team_sizes(const std::vector<int>& tiles, int G) {
         double best_ratio = 1e300;
         for (int i = 0; i < A; ++i) {
             if (P[i] <= 1) continue;
-            double r = (double)tiles[i] / P[i];
+            double r = weight[i] / P[i];
             if (r < best_ratio) { best_ratio = r; best = i; }
         }
         if (best < 0) break;
@@ -1009,21 +1279,55 @@ std::vector<int> team_sizes(const std::vector<int>& tiles, int G) {
 }
 
 template <typename T>
-int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t stream, bool sync) {
-    if (e->broken) return PHS_ERR_STATE;
-    if (n_steps <= 0) return PHS_OK;
-    int occ = 0;
-    int rc = occupancy_for<T>(&occ);
-    if (rc != PHS_OK) return rc;
-    if (occ < 1) return PHS_ERR_CUDA;
-    int cps = (ctas_per_sm > 0) ? std::min(ctas_per_sm, occ) : occ;
+int variant_of(const phs_engine* e) {
+    if (e->variant >= 0) return e->variant;
+    return sizeof(T) == 8 ? kDefaultF64 : kDefaultF32;
+}
+
+void drop_graphs(phs_engine* e) {
+    for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    e->graphs.clear();
+}
+
+template <typename T>
+cudaError_t launch_waves(phs_engine* e, long long n_steps, cudaStream_t stream) {
+    for (auto& wv : e->waves) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)wv.second);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const InstDev<T>* dd = (const InstDev<T>*)e->d_desc;
+        const int4* mp = e->d_map + wv.first;
+        long long ns = n_steps;
+        unsigned int* ab = e->abort_word;
+        void* args[] = {(void*)&dd, (void*)&mp, (void*)&ns, (void*)&ab};
+        cudaError_t ce = cudaLaunchKernelExC(&cfg, step_fn<T>(variant_of<T>(e)), args);
+        if (ce != cudaSuccess) return ce;
+    }
+    return cudaSuccess;
+}
+
+// (Re)build the launch plan: device descriptors, team map and waves.
+template <typename T>
+int build_plan(phs_engine* e, int cps) {
+    // earlier launches may still read the old descriptors
+    PHS_CUDA_TRY(cudaDeviceSynchronize());
     const int G = e->sms * cps;
     std::vector<int> act;
     for (size_t i = 0; i < e->inst.size(); ++i)
         if (e->inst[i].used && !e->inst[i].finished) act.push_back((int)i);
+    e->act = act;
+    e->waves.clear();
+    drop_graphs(e);
+    e->plan_cps = cps;
+    e->dirty = false;
     if (act.empty()) return PHS_OK;
-
-    // descriptors of all active instances
     std::vector<InstDev<T>> descs;
     descs.reserve(act.size());
     for (int i : act) descs.push_back(make_dev<T>(e->inst[i]));
@@ -1033,16 +1337,24 @@ int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t
         PHS_CUDA_TRY(cudaMalloc(&e->d_desc, bytes));
         e->d_desc_bytes = bytes;
     }
-    PHS_CUDA_TRY(cudaMemcpyAsync(e->d_desc, descs.data(), bytes, cudaMemcpyHostToDevice, stream));
+    PHS_CUDA_TRY(cudaMemcpy(e->d_desc, descs.data(), bytes, cudaMemcpyHostToDevice));
 
     // waves of at most G instances
     std::vector<int4> map_all;
-    std::vector<std::pair<size_t, int>> waves;  // (offset into map, grid)
+    std::vector<std::pair<size_t, int>>& waves = e->waves;  // (offset into map, grid)
     for (size_t w0 = 0; w0 < act.size(); w0 += (size_t)G) {
         size_t w1 = std::min(act.size(), w0 + (size_t)G);
         std::vector<int> tiles;
-        for (size_t i = w0; i < w1; ++i) tiles.push_back(e->inst[act[i]].n_tiles);
-        std::vector<int> P = team_sizes(tiles, G);
+        std::vector<double> weight;
+        bool measured = true;
+        for (size_t i = w0; i < w1; ++i) measured = measured && e->inst[act[i]].weight > 0.0;
+        for (size_t i = w0; i < w1; ++i) {
+            const InstHost& h = e->inst[act[i]];
+            tiles.push_back(h.n_tiles);
+            weight.push_back(measured ? h.weight : (double)h.n * (1.6 + h.kavg));
+        }
+        std::vector<int> P = team_sizes(tiles, weight, G);
+        for (size_t i = w0; i < w1; ++i) e->inst[act[i]].team = P[i - w0];
         size_t off = map_all.size();
         int grid = 0;
         for (size_t i = w0; i < w1; ++i) {
@@ -1057,29 +1369,59 @@ int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t
         PHS_CUDA_TRY(cudaMalloc(&e->d_map, map_all.size() * sizeof(int4)));
         e->d_map_n = map_all.size();
     }
-    PHS_CUDA_TRY(cudaMemcpyAsync(e->d_map, map_all.data(), map_all.size() * sizeof(int4),
-                                 cudaMemcpyHostToDevice, stream));
-    for (auto& wv : waves) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)wv.second);
-        cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        const InstDev<T>* dd = (const InstDev<T>*)e->d_desc;
-        const int4* mp = e->d_map + wv.first;
-        cudaError_t ce;
-        if (sizeof(T) == 8)
-            ce = cudaLaunchKernelEx(&cfg, step_kernel<T, kVptF64>, dd, mp, (long long)n_steps, e->abort_word);
-        else
-            ce = cudaLaunchKernelEx(&cfg, step_kernel<T, kVptF32>, dd, mp, (long long)n_steps, e->abort_word);
-        if (ce != cudaSuccess) { set_last_error("launch step_kernel", ce); return PHS_ERR_CUDA; }
-        e->launches += 1;
+    PHS_CUDA_TRY(cudaMemcpy(e->d_map, map_all.data(), map_all.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    return PHS_OK;
+}
+
+template <typename T>
+int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t stream, bool sync) {
+    if (e->broken) return PHS_ERR_STATE;
+    if (n_steps <= 0) return PHS_OK;
+    int occ = 0;
+    int rc = occupancy_for<T>(&occ, variant_of<T>(e));
+    if (rc != PHS_OK) return rc;
+    if (occ < 1) return PHS_ERR_CUDA;
+    if (ctas_per_sm <= 0) ctas_per_sm = e->default_cps;
+    int cps = (ctas_per_sm > 0) ? std::min(ctas_per_sm, occ) : occ;
+    if (e->dirty || cps != e->plan_cps) {
+        rc = build_plan<T>(e, cps);
+        if (rc != PHS_OK) return rc;
     }
+    const std::vector<int>& act = e->act;
+    if (act.empty()) return PHS_OK;
+    cudaError_t ce = cudaSuccess;
+    bool launched = false;
+    if (stream != nullptr && e->graphs_ok) {
+        auto it = e->graphs.find(n_steps);
+        if (it == e->graphs.end()) {
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t ge = nullptr;
+            ce = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+            if (ce == cudaSuccess) {
+                cudaError_t le = launch_waves<T>(e, n_steps, stream);
+                ce = cudaStreamEndCapture(stream, &g);
+                if (le != cudaSuccess) ce = le;
+            }
+            if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ge, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (ce == cudaSuccess) {
+                it = e->graphs.emplace(n_steps, ge).first;
+            } else {
+                cudaGetLastError();  // clear; fall back to direct launches
+                e->graphs_ok = false;
+            }
+        }
+        if (e->graphs_ok) {
+            ce = cudaGraphLaunch(it->second, stream);
+            if (ce != cudaSuccess) { set_last_error("cudaGraphLaunch", ce); return PHS_ERR_CUDA; }
+            launched = true;
+        }
+    }
+    if (!launched) {
+        ce = launch_waves<T>(e, n_steps, stream);
+        if (ce != cudaSuccess) { set_last_error("launch step_kernel", ce); return PHS_ERR_CUDA; }
+    }
+    e->launches += (long long)e->waves.size();
     if (!sync) return PHS_OK;
     PHS_CUDA_TRY(cudaStreamSynchronize(stream));
     unsigned int ab = 0;
@@ -1089,7 +1431,10 @@ int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t
     for (int i : act) {
         InstHost& h = e->inst[i];
         PHS_CUDA_TRY(cudaMemcpy(&h.st_host, h.st, sizeof(InstState), cudaMemcpyDeviceToHost));
-        if (h.st_host.step >= h.d.n_steps || h.st_host.status == PHS_ERR_NONFINITE) h.finished = true;
+        if (h.st_host.step >= h.d.n_steps || h.st_host.status == PHS_ERR_NONFINITE) {
+            if (!h.finished) e->dirty = true;
+            h.finished = true;
+        }
         if (h.st_host.status == PHS_ERR_NONFINITE) worst = PHS_ERR_NONFINITE;
         else if (h.st_host.status == PHS_WARN_NO_CONVERGE && worst == PHS_OK) worst = PHS_WARN_NO_CONVERGE;
     }
@@ -1107,7 +1452,8 @@ int phs_device_query(int precision, int* sm_count, int* ctas_per_sm) {
     int sms = 0;
     PHS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     int occ = 0;
-    int rc = (precision == PHS_PREC_F64) ? occupancy_for<double>(&occ) : occupancy_for<float>(&occ);
+    int rc = (precision == PHS_PREC_F64) ? occupancy_for<double>(&occ, kDefaultF64)
+                                         : occupancy_for<float>(&occ, kDefaultF32);
     if (rc != PHS_OK) return rc;
     if (sm_count) *sm_count = sms;
     if (ctas_per_sm) *ctas_per_sm = occ;
@@ -1135,6 +1481,7 @@ int phs_engine_create(int precision, phs_engine** out) {
 int phs_engine_destroy(phs_engine* e) {
     if (!e) return PHS_ERR_BAD_ARG;
     cudaDeviceSynchronize();
+    drop_graphs(e);
     for (auto& h : e->inst)
         if (h.used) free_inst(h);
     if (e->abort_word) cudaFree(e->abort_word);
@@ -1153,6 +1500,7 @@ int phs_instance_remove(phs_engine* e, int slot) {
     if (!e || slot < 0 || slot >= (int)e->inst.size() || !e->inst[slot].used) return PHS_ERR_BAD_ARG;
     cudaDeviceSynchronize();
     free_inst(e->inst[slot]);
+    e->dirty = true;
     return PHS_OK;
 }
 
@@ -1169,6 +1517,7 @@ int phs_instance_info_get(phs_engine* e, int slot, phs_instance_info* info) {
     info->solves = h.st_host.solves;
     info->max_arnoldi = h.st_host.max_arnoldi;
     info->nonconverged = h.st_host.nonconv;
+    info->arnoldi_sq = h.st_host.arnoldi_sq;
     return PHS_OK;
 }
 
@@ -1219,6 +1568,92 @@ int phs_instance_device_ptrs(phs_engine* e, int slot, void** u, void** hist_u, i
 }
 
 int64_t phs_engine_launch_count(phs_engine* e) { return e ? e->launches : -1; }
+
+int phs_engine_rebalance(phs_engine* e) {
+    if (!e) return PHS_ERR_BAD_ARG;
+    PHS_CUDA_TRY(cudaDeviceSynchronize());
+    for (auto& h : e->inst) {
+        if (!h.used) continue;
+        PHS_CUDA_TRY(cudaMemcpy(&h.st_host, h.st, sizeof(InstState), cudaMemcpyDeviceToHost));
+        const long long ds = h.st_host.step - h.ref_step;
+        if (ds > 0) h.kavg = (double)(h.st_host.arnoldi - h.ref_arnoldi) / (double)ds;
+        h.ref_step = h.st_host.step;
+        h.ref_arnoldi = h.st_host.arnoldi;
+        // measured cost: the team's time per step times its CTAs
+        h.weight = 0.0;
+        if (h.prof) {
+            unsigned long long pf[kProfSlots];
+            PHS_CUDA_TRY(cudaMemcpy(pf, h.prof, sizeof(pf), cudaMemcpyDeviceToHost));
+            const unsigned long long steps = pf[PF_STEPS] - h.prof_ref[PF_STEPS];
+            unsigned long long ns = 0;
+            for (int i = 0; i <= PF_STEP_WAIT; ++i) ns += pf[i] - h.prof_ref[i];
+            if (steps > 0 && h.team > 0) h.weight = (double)ns / (double)steps * (double)h.team;
+            for (int i = 0; i < kProfSlots; ++i) h.prof_ref[i] = pf[i];
+        }
+    }
+    e->dirty = true;
+    return PHS_OK;
+}
+
+int phs_instance_profile(phs_engine* e, int slot, uint64_t* out16) {
+    if (!e || !out16 || slot < 0 || slot >= (int)e->inst.size() || !e->inst[slot].used) return PHS_ERR_BAD_ARG;
+    InstHost& h = e->inst[slot];
+    if (!h.prof) return PHS_ERR_STATE;
+    PHS_CUDA_TRY(cudaDeviceSynchronize());
+    PHS_CUDA_TRY(cudaMemcpy(out16, h.prof, kProfSlots * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    return PHS_OK;
+}
+
+int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, int32_t* max_regs) {
+    if (precision != PHS_PREC_F32 && precision != PHS_PREC_F64) return PHS_ERR_BAD_ARG;
+    const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
+    if (count) *count = nv;
+    for (int v = 0; v < nv; ++v) {
+        if (min_ctas_per_sm) min_ctas_per_sm[v] = precision == PHS_PREC_F64 ? kMinbF64[v] : kMinbF32[v];
+        if (max_regs) {
+            cudaFuncAttributes a{};
+            const void* fn = precision == PHS_PREC_F64 ? step_fn<double>(v) : step_fn<float>(v);
+            max_regs[v] = (cudaFuncGetAttributes(&a, fn) == cudaSuccess) ? a.numRegs : -1;
+        }
+    }
+    return PHS_OK;
+}
+
+int phs_engine_config(phs_engine* e, int key, int64_t value) {
+    if (!e) return PHS_ERR_BAD_ARG;
+    switch (key) {
+        case PHS_CFG_VARIANT: {
+            const int nv = e->prec == PHS_PREC_F64 ? kNumF64 : kNumF32;
+            if (value < -1 || value >= nv) return PHS_ERR_BAD_ARG;
+            if (e->variant != (int)value) {
+                e->variant = (int)value;
+                e->dirty = true;
+            }
+            return PHS_OK;
+        }
+        case PHS_CFG_CTAS_PER_SM:
+            if (value < 0 || value > 32) return PHS_ERR_BAD_ARG;
+            e->default_cps = (int)value;
+            return PHS_OK;
+        case PHS_CFG_PROFILE:
+            cudaDeviceSynchronize();
+            e->profile = value != 0;
+            for (auto& h : e->inst) {
+                if (!h.used) continue;
+                if (e->profile && !h.prof) {
+                    if (cudaMalloc((void**)&h.prof, kProfSlots * sizeof(unsigned long long)) != cudaSuccess)
+                        return PHS_ERR_OOM;
+                }
+                if (h.prof) cudaMemset(h.prof, 0, kProfSlots * sizeof(unsigned long long));
+                if (!e->profile && h.prof) { cudaFree(h.prof); h.prof = nullptr; }
+                for (int i = 0; i < kProfSlots; ++i) h.prof_ref[i] = 0;
+            }
+            e->dirty = true;
+            return PHS_OK;
+        default:
+            return PHS_ERR_BAD_ARG;
+    }
+}
 
 int phs_simulate(const phs_instance_desc* desc, int precision, void* u_hist, void* h_hist, int32_t* lat,
                  int32_t* n_saved, phs_instance_info* info) {

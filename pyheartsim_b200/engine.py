@@ -1,0 +1,140 @@
+"""Batched engine: many uneven simulation instances advanced together.
+
+Thin Python handle over the ``phs_engine_*`` C ABI (include/phs.h).  Each call
+to :meth:`advance` is one persistent sm_100a launch in which every unfinished
+instance is advanced by a team of CTAs sized to its voxel count; instances of
+different sizes, models and time steps progress independently.  State, solver
+workspace, stimulus schedule and history stay on the device between calls.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+class BatchedEngine:
+    def __init__(self, precision=_lib.PREC_F32):
+        self.precision = precision
+        self._h = ctypes.c_void_p()
+        _lib.check(_lib.lib().phs_engine_create(precision, ctypes.byref(self._h)), "phs_engine_create")
+        self._inst = {}
+
+    # -- instances ------------------------------------------------------------
+    def add(self, inst):
+        """Upload a :class:`pyheartsim_b200.instance.CompiledInstance`; returns its slot."""
+        slot = ctypes.c_int(-1)
+        desc = inst.desc()
+        _lib.check(_lib.lib().phs_instance_add(self._h, ctypes.byref(desc), ctypes.byref(slot)), "phs_instance_add")
+        self._inst[slot.value] = inst
+        return slot.value
+
+    def remove(self, slot):
+        _lib.check(_lib.lib().phs_instance_remove(self._h, slot), "phs_instance_remove")
+        self._inst.pop(slot, None)
+
+    def instance(self, slot):
+        return self._inst[slot]
+
+    def slots(self):
+        return list(self._inst)
+
+    # -- stepping ---------------------------------------------------------------
+    def advance(self, n_steps, stream=None, sync=True, ctas_per_sm=0):
+        """Advance every unfinished instance by up to ``n_steps`` steps.
+
+        ``stream`` is a cudaStream_t handle (int) or a torch.cuda.Stream.
+        Returns the worst instance status (OK or the no-convergence warning)."""
+        if stream is not None and hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        st = _lib.lib().phs_engine_advance(self._h, int(n_steps), int(ctas_per_sm),
+                                           ctypes.c_void_p(stream) if stream else None, 1 if sync else 0)
+        return _lib.check(st, "phs_engine_advance", allow_warn=True)
+
+    def info(self, slot):
+        i = _lib.InstanceInfo()
+        _lib.check(_lib.lib().phs_instance_info_get(self._h, slot, ctypes.byref(i)), "phs_instance_info_get")
+        return {k: getattr(i, k) for k, _ in _lib.InstanceInfo._fields_}
+
+    def finished(self, slot):
+        i = self.info(slot)
+        return i["step"] >= i["n_steps"] or i["status"] == _lib.PHS_ERR_NONFINITE
+
+    # -- results ----------------------------------------------------------------
+    def history(self, slot, s0=0, count=None, with_h=False):
+        inst = self._inst[slot]
+        info = self.info(slot)
+        if count is None:
+            count = info["samples"] - s0
+        dt = _lib.np_dtype(self.precision)
+        u = np.empty((count, inst.n_voxel), dtype=dt)
+        h = np.empty((count, inst.n_voxel), dtype=dt) if with_h else None
+        _lib.check(_lib.lib().phs_instance_read_history(self._h, slot, s0, count, _lib.vptr(u), _lib.vptr(h)),
+                   "phs_instance_read_history")
+        return (u, h) if with_h else u
+
+    def state(self, slot):
+        inst = self._inst[slot]
+        dt = _lib.np_dtype(self.precision)
+        u = np.empty(inst.n_voxel, dtype=dt)
+        h = np.empty(inst.n_voxel, dtype=dt)
+        lat = np.empty(inst.n_voxel, dtype=np.int32)
+        _lib.check(_lib.lib().phs_instance_read_state(self._h, slot, _lib.vptr(u), _lib.vptr(h),
+                                                      _lib.ptr(lat, ctypes.c_int32)), "phs_instance_read_state")
+        return u, h, lat
+
+    def configure(self, variant=None, ctas_per_sm=None):
+        """Select the step-kernel variant and the CTAs per SM used by advance()."""
+        L = _lib.lib()
+        if variant is not None:
+            _lib.check(L.phs_engine_config(self._h, _lib.CFG_VARIANT, int(variant)), "phs_engine_config")
+        if ctas_per_sm is not None:
+            _lib.check(L.phs_engine_config(self._h, _lib.CFG_CTAS_PER_SM, int(ctas_per_sm)), "phs_engine_config")
+
+    def rebalance(self):
+        """Re-split CTAs over instances by recent cost (voxels x Arnoldi iterations)."""
+        _lib.check(_lib.lib().phs_engine_rebalance(self._h), "phs_engine_rebalance")
+
+    def set_profile(self, on=True):
+        _lib.check(_lib.lib().phs_engine_config(self._h, _lib.CFG_PROFILE, 1 if on else 0), "phs_engine_config")
+
+    def profile(self, slot):
+        """Phase timers of an instance in ms (team's first CTA), plus counts."""
+        out = (ctypes.c_uint64 * 16)()
+        _lib.check(_lib.lib().phs_instance_profile(self._h, slot, out), "phs_instance_profile")
+        d = {}
+        for i, name in enumerate(_lib.PROFILE_SLOTS):
+            d[name] = int(out[i]) if name in ("steps", "arnoldi_iters", "team_ctas") else out[i] / 1e6
+        return d
+
+    def launches(self):
+        return int(_lib.lib().phs_engine_launch_count(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.lib().phs_engine_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._inst.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def step_variants(precision=_lib.PREC_F32):
+    """[(variant, min CTAs/SM it was compiled for, registers per thread)]."""
+    n = ctypes.c_int32(0)
+    _lib.check(_lib.lib().phs_step_variants(precision, ctypes.byref(n), None, None), "phs_step_variants")
+    minb = np.zeros(n.value, dtype=np.int32)
+    regs = np.zeros(n.value, dtype=np.int32)
+    _lib.check(_lib.lib().phs_step_variants(precision, ctypes.byref(n), _lib.ptr(minb, ctypes.c_int32),
+                                            _lib.ptr(regs, ctypes.c_int32)), "phs_step_variants")
+    return [(i, int(minb[i]), int(regs[i])) for i in range(n.value)]

@@ -34,7 +34,7 @@ def test_bindings_cover_header():
 def test_struct_layouts_match_c():
     # sizes fixed by include/phs.h (natural alignment, 64-bit)
     assert ctypes.sizeof(_lib.InstanceDesc) == 184
-    assert ctypes.sizeof(_lib.InstanceInfo) == 56
+    assert ctypes.sizeof(_lib.InstanceInfo) == 64
 
 
 def test_status_strings_without_gpu():
