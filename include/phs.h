@@ -189,6 +189,18 @@ int64_t phs_egm_bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
 int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
                             const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi,
                             const uint16_t* Mlo, float* egm, void* work, void* stream);
+/* Allocation-free form of phs_egm_contract_f64 (no counterpart in the reference).
+ * For callers that cannot allocate device memory when they contract: inside a
+ * global-mode stream capture, under another allocator that owns the device
+ * memory, or in loops that cannot absorb cudaFree's device-wide synchronisation.
+ * Same inputs and result as phs_egm_contract_f64; its split-K partial sums live
+ * in a fixed 16 MiB device array (phs_egm_noalloc_capacity() doubles) inside the
+ * library, so T * n_e must not exceed that capacity (else PHS_ERR_BAD_ARG).  The
+ * first call on a device looks up the array's address: make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race. */
+int phs_egm_contract_f64_noalloc(int64_t T, int64_t n_v, int64_t n_e, const double* V, int64_t ldv,
+                                 const double* Mt, double* egm, void* stream);
+int64_t phs_egm_noalloc_capacity(void);
 /* Scale egm ([T][n_e], f64 or f32 per is_f64) in place by 1/mean_e(max_t - min_t),
  * simulation/unipolar_electrogram_equation_parts.py:118-124.                      */
 int phs_egm_normalize(int64_t T, int64_t n_e, void* egm, int is_f64, void* stream);

@@ -129,6 +129,10 @@ SIGNATURES = {
     "phs_egm_contract_bf16x3": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                                ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_egm_contract_f64_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+                                                    ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_void_p]),
+    "phs_egm_noalloc_capacity": (ctypes.c_int64, []),
     "phs_egm_normalize": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.c_void_p]),
     "phs_electrogram": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_double_p, c_double_p,

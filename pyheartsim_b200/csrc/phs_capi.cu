@@ -17,6 +17,11 @@ void set_last_error(const char* where, cudaError_t e) {
     std::lock_guard<std::mutex> lk(g_err_mu);
     snprintf(g_err, sizeof(g_err), "%s: %s (%s)", where, cudaGetErrorName(e), cudaGetErrorString(e));
 }
+
+void set_last_message(const char* msg) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    snprintf(g_err, sizeof(g_err), "%s", msg);
+}
 }  // namespace phs
 
 extern "C" {

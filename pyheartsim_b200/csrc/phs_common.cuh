@@ -13,6 +13,8 @@ constexpr int kPhaseScalars = 4;
 
 // Record a CUDA error message (host side); defined in phs_capi.cu.
 void set_last_error(const char* where, cudaError_t e);
+// Record a plain error message for phs_last_error().
+void set_last_message(const char* msg);
 
 }  // namespace phs
 

@@ -178,6 +178,32 @@ int contract_f64(int64_t T, int64_t n_v, int64_t n_e, const double* V, int64_t l
     return PHS_OK;
 }
 
+// Launch the split-K FP64 contraction into caller-provided partials
+// P[splits][T][n_e] and reduce them into egm (used by the allocation-free entry
+// point in phs_noalloc.cu).  `max_partials` bounds splits * T * n_e.
+int contract_f64_into(int64_t T, int64_t n_v, int64_t n_e, const double* V, int64_t ldv, const double* Mt,
+                      double* egm, double* P, int64_t max_partials, cudaStream_t stream) {
+    if (T <= 0 || n_v <= 0 || n_e <= 0 || ldv < n_v || T * n_e > max_partials) return PHS_ERR_BAD_ARG;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t tm = (T + DG_BM - 1) / DG_BM, tn = (n_e + DG_BN - 1) / DG_BN;
+    const int64_t target = 2LL * sms;
+    int64_t splits = std::max<int64_t>(1, std::min<int64_t>((target + tm * tn - 1) / (tm * tn), (n_v + 255) / 256));
+    splits = std::min<int64_t>(splits, max_partials / (T * n_e));
+    int64_t kchunk = (n_v + splits - 1) / splits;
+    kchunk = ((kchunk + DG_BK - 1) / DG_BK) * DG_BK;
+    splits = (n_v + kchunk - 1) / kchunk;
+    dim3 grid((unsigned)tm, (unsigned)tn, (unsigned)splits);
+    dgemm_tn_kernel<<<grid, 256, 0, stream>>>(T, n_e, n_v, V, ldv, Mt, n_v, P, kchunk);
+    const int64_t MN = T * n_e;
+    splitk_reduce_kernel<double><<<(unsigned)std::min<int64_t>((MN + 255) / 256, 4096), 256, 0, stream>>>(
+        MN, (int)splits, P, egm);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { set_last_error("contract_f64_into", e); return PHS_ERR_CUDA; }
+    return PHS_OK;
+}
+
 int normalize(int64_t T, int64_t n_e, void* egm, bool is_f64, cudaStream_t stream) {
     double* ptp = nullptr;
     PHS_CUDA_TRY(cudaMallocAsync((void**)&ptp, (size_t)n_e * sizeof(double), stream));
