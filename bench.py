@@ -51,6 +51,11 @@ def parse():
     p.add_argument("--no-extras", action="store_true", help="skip e2e, plain-FP64, accuracy and CPU legs")
     p.add_argument("--no-tune", action="store_true", help="use the default step-kernel variant")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--serving-requests", type=int, default=16)
+    p.add_argument("--egm-nv", type=int, default=500_000)
+    p.add_argument("--egm-ne", type=int, default=2048)
+    p.add_argument("--egm-T", type=int, default=1000)
+    p.add_argument("--egm-only", action="store_true", help="run only the electrogram leg (profiling case)")
     return p.parse_args()
 
 
@@ -268,6 +273,9 @@ def run_b200(args):
         if rank == 0 and world == 1:
             line["plain_fp64"] = plain_leg(args, batch, value, dev)
             line["accuracy"] = accuracy_leg(dev, args.tol)
+            del batch, insts
+            line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
+            line["electrogram"] = egm_leg(args, dev)
             line["cpu_baseline"] = cpu_leg(args)
     if world > 1:
         import torch.distributed as dist
@@ -383,6 +391,130 @@ def accuracy_leg(dev, tol):
             "max_abs_dvm": float(np.abs(u64 - u32).max()), "voxels": int(n), "ms": 60.0, "tol": tol}
 
 
+def serving_leg(args, plain_rate, dev):
+    """Continuous batching under Poisson arrivals (20/s, 20k-1M voxels, 200-2000 ms,
+    random model and pacing site): latency percentiles and served throughput.
+    The plain-FP64-serial comparison is an estimate from the measured plain rate
+    (running it for real would take hours)."""
+    import torch
+    from pyheartsim_b200 import serving
+    reqs = serving.poisson_requests(args.serving_requests, seed=args.seed)
+    free = torch.cuda.mem_get_info(dev)[0]
+    srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
+                         stream=torch.cuda.current_stream(dev).cuda_stream)
+    done, totals = srv.run(reqs)
+    srv.close()
+    out = serving.summarize(done, totals, reqs)
+    # FIFO single-server schedule of the same requests at the plain FP64 rate
+    t = 0.0
+    lat = []
+    for r in sorted(done, key=lambda r: r.arrival_s):
+        t = max(t, r.arrival_s) + r.inst.n_voxel * r.inst.n_steps / plain_rate
+        lat.append(t - r.arrival_s)
+    out["plain_fp64_serial_estimate"] = {"p50_latency_s": float(np.percentile(lat, 50)),
+                                         "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": t}
+    return out
+
+
+def egm_leg(args, dev, history=None):
+    """Electrogram contraction at its configured size: lead field of n_e seeded
+    electrodes 2 mm off an n_v-voxel shell (FP64, on device), Vm history of T
+    samples from an S1-S2 run of the FP32 engine, BF16 hi/lo x3 on tcgen05 vs the
+    FP64 contraction."""
+    import ctypes
+    import torch
+    from pyheartsim_b200 import _lib, synthetic, workloads
+    from pyheartsim_b200.engine import BatchedEngine
+    from pyheartsim_b200.geometry import lattice_neighbors
+    from pyheartsim_b200.instance import compile_instance
+    from pyheartsim_b200.simulation.unipolar_electrogram_gpu import incoming_gradient_terms
+    L = _lib.lib()
+    rng = np.random.default_rng(args.seed + 4)
+    ijk = workloads._shell_scaled(args.egm_nv, args.seed + 4)
+    nb = lattice_neighbors(ijk)
+    n_v, n_e, T = ijk.shape[0], args.egm_ne, args.egm_T
+    xyz = ijk * 0.4
+    x = ijk[:, 0]
+    s1 = np.where(x <= x.min() + 3)[0]
+    s2 = np.where((x < np.median(x)) & (ijk[:, 1] > np.median(ijk[:, 1])))[0]
+    case = synthetic.make_case(ijk, 0.4, 0, 0.05, float(T), s1, s2_ids=s2, flag=1, s1_s2=250.0)
+    inst = compile_instance(*case, full_cycles=False, tol=1e-7, restart=20, save_h=False)
+    eng = BatchedEngine(_lib.PREC_F32)
+    slot = eng.add(inst)
+    t0 = time.perf_counter()
+    while not eng.finished(slot):
+        eng.advance(2000, sync=True)
+    sim_s = time.perf_counter() - t0
+    samples = eng.info(slot)["samples"]
+    T = min(T, samples)
+    # the history stays on the device: read it back into a torch tensor
+    Vf32 = torch.from_numpy(eng.history(slot, 0, T)).to(dev)
+    eng.close()
+    el = synthetic.electrodes_off_surface(ijk, 0.4, n_e, rng)
+    c = torch.tensor(case[1][:, 20], dtype=torch.float64, device=dev)
+    ptr, srcv, dirs = incoming_gradient_terms(nb)
+    dxyz = torch.tensor(xyz, dtype=torch.float64, device=dev)
+    dex = torch.tensor(el, dtype=torch.float64, device=dev)
+    dptr = torch.tensor(ptr, device=dev)
+    dsrc = torch.tensor(srcv, device=dev)
+    ddir = torch.tensor(dirs, device=dev)
+    Mt = torch.empty((n_e, n_v), dtype=torch.float64, device=dev)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    ev[0].record(stream)
+    _lib.check(L.phs_egm_leadfield_f64(n_v, n_e, p(dxyz), p(dex), p(c), None, p(dptr), p(dsrc), p(ddir),
+                                       1.0 / 0.8, p(Mt), sp), "leadfield")
+    ev[1].record(stream)
+    V64 = Vf32.double()
+    ref = torch.empty((T, n_e), dtype=torch.float64, device=dev)
+    ev[2].record(stream)
+    _lib.check(L.phs_egm_contract_f64(T, n_v, n_e, p(V64), n_v, p(Mt), p(ref), sp), "contract_f64")
+    ev[3].record(stream)
+    Tp, Ep, Kp = (T + 127) // 128 * 128, (n_e + 127) // 128 * 128, (n_v + 63) // 64 * 64
+    vh = torch.empty((Tp, Kp), dtype=torch.uint16, device=dev)
+    vl = torch.empty_like(vh)
+    mh = torch.empty((Ep, Kp), dtype=torch.uint16, device=dev)
+    ml = torch.empty_like(mh)
+    _lib.check(L.phs_split_bf16(T, n_v, p(Vf32), n_v, 0, p(vh), p(vl), Tp, Kp, sp), "split V")
+    _lib.check(L.phs_split_bf16(n_e, n_v, p(Mt), n_v, 1, p(mh), p(ml), Ep, Kp, sp), "split M")
+    work = torch.empty(L.phs_egm_bf16x3_workspace(Tp, Ep, Kp), dtype=torch.uint8, device=dev)
+    out = torch.empty((T, n_e), dtype=torch.float32, device=dev)
+    reps = 3
+    for _ in range(2):          # warm-up
+        _lib.check(L.phs_egm_contract_bf16x3(T, n_e, Tp, Ep, Kp, p(vh), p(vl), p(mh), p(ml), p(out), p(work), sp),
+                   "contract_bf16x3")
+    ev[4].record(stream)
+    for _ in range(reps):
+        _lib.check(L.phs_egm_contract_bf16x3(T, n_e, Tp, Ep, Kp, p(vh), p(vl), p(mh), p(ml), p(out), p(work), sp),
+                   "contract_bf16x3")
+    ev[5].record(stream)
+    torch.cuda.synchronize()
+    ms_bf = ev[4].elapsed_time(ev[5]) / reps
+    ms_f64 = ev[2].elapsed_time(ev[3])
+    flops = 2.0 * T * n_e * n_v
+    pk, pk_src = peaks()
+    r = ref.cpu().numpy()
+    o = out.double().cpu().numpy()
+    rel = float(np.linalg.norm(o - r) / np.linalg.norm(r))
+    # the same BF16 parts multiplied exactly in FP64: separates the split's
+    # representation error from the kernel's accumulation
+    b = lambda t: t.view(torch.bfloat16)[:, :n_v].double()
+    ideal = (b(vh)[:T] @ b(mh)[:n_e].T + b(vh)[:T] @ b(ml)[:n_e].T + b(vl)[:T] @ b(mh)[:n_e].T).cpu().numpy()
+    rel_ideal = float(np.linalg.norm(ideal - r) / np.linalg.norm(r))
+    rel_kernel = float(np.linalg.norm(o - ideal) / np.linalg.norm(r))
+    tf_exec = 3 * flops / (ms_bf / 1e3) / 1e12
+    return {"config": {"voxels": int(n_v), "electrodes": int(n_e), "samples": int(T),
+                       "history": "S1-S2 run of the FP32 engine (Mitchell-Schaeffer, S2 at 250 ms)",
+                       "simulation_s": sim_s},
+            "bf16x3_ms": ms_bf, "useful_tflops": flops / (ms_bf / 1e3) / 1e12, "executed_tflops": tf_exec,
+            "tensor_frac": tf_exec / pk["bf16_tflops"], "peak_tflops": pk["bf16_tflops"], "peak_source": pk_src,
+            "fp64_contract_ms": ms_f64, "fp64_tflops": flops / (ms_f64 / 1e3) / 1e12,
+            "leadfield_ms": ev[0].elapsed_time(ev[1]), "rel_l2_bf16x3_vs_fp64": rel,
+            "rel_l2_exact_product_of_parts": rel_ideal, "rel_l2_kernel_vs_exact_parts": rel_kernel}
+
+
 def cpu_leg(args):
     """Port of the reference's legacy CPU stepper on the median MS instance,
     bounded to ``--cpu-seconds`` of stepping after JIT warm-up."""
@@ -408,6 +540,12 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.egm_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"electrogram": egm_leg(args, dev)}), flush=True)
+        return 0
     return run_b200(args)
 
 

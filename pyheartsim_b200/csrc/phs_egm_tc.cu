@@ -262,15 +262,15 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
     }
 }
 
-// egm[t][e] = sum_z part[z][t][e] (split order), t < T, e < n_e.
+// egm[t][e] = sum_z part[z][t][e] (split order, FP64), t < T, e < n_e.
 __global__ void tc_reduce_kernel(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int splits,
                                  const float* __restrict__ part, float* __restrict__ egm) {
     const int64_t total = T * n_e;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = i / n_e, e = i % n_e;
-        float s = 0.0f;
-        for (int z = 0; z < splits; ++z) s += part[((size_t)z * T_pad + t) * E_pad + e];
-        egm[i] = s;
+        double s = 0.0;
+        for (int z = 0; z < splits; ++z) s += (double)part[((size_t)z * T_pad + t) * E_pad + e];
+        egm[i] = (float)s;
     }
 }
 
@@ -319,6 +319,12 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k) {
     return r == CUDA_SUCCESS;
 }
 
+// Split-K: at least ~4 CTAs per SM, and at most kMaxKBlocksPerSplit K blocks
+// accumulated in one FP32 TMEM accumulator.  Long FP32 accumulation chains are
+// the dominant error of the split-BF16 contraction (the dipole sum cancels), so
+// each accumulator is kept short and the slices are summed in FP64.
+constexpr int64_t kMaxKBlocksPerSplit = 128;
+
 void splits_for(int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* kb_per) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -326,7 +332,9 @@ void splits_for(int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* k
     const int64_t tiles = (T_pad / TC_BM) * (E_pad / TC_BN);
     const int64_t nkb = K_pad / TC_BK;
     int64_t s = std::max<int64_t>(1, (4LL * sms + tiles - 1) / tiles);
+    s = std::max<int64_t>(s, (nkb + kMaxKBlocksPerSplit - 1) / kMaxKBlocksPerSplit);
     s = std::min<int64_t>(s, std::max<int64_t>(1, nkb / 8));
+    s = std::min<int64_t>(s, 65535);
     int64_t per = (nkb + s - 1) / s;
     s = (nkb + per - 1) / per;
     *splits = (int)s;

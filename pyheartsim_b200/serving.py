@@ -1,0 +1,183 @@
+"""Continuous-batching server for simulation requests.
+
+Requests (a geometry size, a model, a simulated duration, a pacing site) arrive
+over time.  The server keeps one FP32 :class:`BatchedEngine` on the GPU and,
+between launches,
+
+* admits waiting requests in arrival order while their device footprint fits
+  the HBM budget (FIFO: the head of the queue is never overtaken);
+* advances every admitted instance by ``steps_per_launch`` steps in one
+  persistent launch (instances of different sizes and models share it, each
+  with its own team of CTAs, so new requests overlap with running ones);
+* retires instances that reached their last step: reads the 1 kHz Vm history
+  back, frees their device memory and lets the next request in;
+* re-splits CTAs over the running instances by measured cost every
+  ``rebalance_every`` launches.
+
+Request inputs are compiled on host threads while the GPU runs.  Because the
+engine's reductions do not depend on team size or batch-mates, every result is
+bit-identical to running the same request alone.
+"""
+import math
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+from . import _lib, workloads
+from .engine import BatchedEngine
+
+
+class Request:
+    def __init__(self, rid, arrival_s, n_target, duration_ms, model, seed):
+        self.rid = rid
+        self.arrival_s = arrival_s
+        self.n_target = int(n_target)
+        self.duration_ms = float(duration_ms)
+        self.model = int(model)
+        self.seed = int(seed)
+        self.inst = None
+        self.future = None
+        self.admit_s = None
+        self.done_s = None
+        self.slot = None
+        self.history = None
+        self.status = None
+
+
+def poisson_requests(count, rate_per_s=20.0, n_min=20_000, n_max=1_000_000, dur_ms=(200.0, 2000.0), seed=0):
+    """Seeded request list: Poisson arrivals, log-uniform sizes, uniform
+    durations, random model (0 MS / 1 AP) and pacing site (per-request seed)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_per_s, size=count))
+    n = np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=count))
+    d = rng.uniform(dur_ms[0], dur_ms[1], size=count)
+    m = rng.integers(0, 2, size=count)
+    return [Request(i, float(t[i]), n[i], d[i], m[i], seed * 100_003 + i) for i in range(count)]
+
+
+def build(req, tol=1e-7, restart=20):
+    """Compile a request into an FP32 early-exit instance (shell geometry with scar)."""
+    i = 2 * (req.seed % 1000) + req.model        # parity of i selects the model in shell_case
+    inst, _, meta = workloads.shell_case(i, req.n_target, req.seed // 1000, t_phys=req.duration_ms, tol=tol,
+                                         restart=restart)
+    return inst
+
+
+def footprint_bytes(inst):
+    """Device bytes of an FP32 instance (tables, state, Krylov basis, history, partials)."""
+    n = inst.n_voxel
+    m = min(inst.restart, n)
+    tiles = math.ceil(n / 1024)
+    per_voxel = 24 + 24 + 1 + 5 * 4 + (m + 1) * 4 + 4 + inst.n_samples * 4 * (2 if inst.save_h else 1)
+    return n * per_voxel + tiles * 8 * (m + 2) * 8 + inst.n_steps + 64 * 1024
+
+
+class _Inline:
+    """Executor that builds requests synchronously (build_threads=0)."""
+
+    def submit(self, fn, *a):
+        from concurrent.futures import Future
+        f = Future()
+        f.set_result(fn(*a))
+        return f
+
+    def shutdown(self, wait=True):
+        pass
+
+
+class Server:
+    def __init__(self, hbm_budget_bytes, steps_per_launch=50, rebalance_every=8, build_threads=8, tol=1e-7,
+                 stream=None, engine=None, builder=None, footprint=None):
+        self.budget = int(hbm_budget_bytes)
+        self.S = int(steps_per_launch)
+        self.rebalance_every = int(rebalance_every)
+        self.tol = tol
+        self.builder = builder or (lambda r: build(r, self.tol))
+        self.footprint = footprint or footprint_bytes
+        self.engine = engine if engine is not None else BatchedEngine(_lib.PREC_F32)
+        self.engine.set_profile(True)
+        self.pool = ThreadPoolExecutor(max_workers=build_threads) if build_threads > 0 else _Inline()
+        self.stream = stream
+        self.used = 0
+        self.launches = 0
+
+    def run(self, requests, keep_history=False, time_scale=1.0, log=None):
+        """Serve ``requests`` (arrival times in seconds, scaled by ``time_scale``)
+        against the wall clock.  Returns per-request records and totals."""
+        reqs = sorted(requests, key=lambda r: r.arrival_s)
+        for r in reqs:
+            r.future = self.pool.submit(self.builder, r)
+        queue = deque()
+        active = {}
+        done = []
+        t0 = time.perf_counter()
+        nxt = 0
+        work = 0.0
+        while nxt < len(reqs) or queue or active:
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt].arrival_s * time_scale <= now:
+                queue.append(reqs[nxt])
+                nxt += 1
+            # FIFO admission under the HBM budget
+            while queue:
+                r = queue[0]
+                if not r.future.done() and active:
+                    break                                  # head still compiling; keep the GPU busy
+                inst = r.future.result()
+                fp = self.footprint(inst)
+                if active and self.used + fp > self.budget:
+                    break
+                queue.popleft()
+                r.inst = inst
+                r.slot = self.engine.add(inst)
+                r.admit_s = time.perf_counter() - t0
+                r.fp = fp
+                self.used += fp
+                active[r.slot] = r
+                if log:
+                    log(f"admit {r.rid} n={inst.n_voxel} steps={inst.n_steps} t={r.admit_s:.2f}")
+            if not active:
+                if nxt < len(reqs):
+                    time.sleep(max(0.0, min(0.05, reqs[nxt].arrival_s * time_scale - now)))
+                continue
+            self.engine.advance(self.S, stream=self.stream, sync=True)
+            self.launches += 1
+            if self.launches % self.rebalance_every == 0:
+                self.engine.rebalance()
+            for slot in list(active):
+                info = self.engine.info(slot)
+                if info["step"] >= info["n_steps"] or info["status"] == _lib.PHS_ERR_NONFINITE:
+                    r = active.pop(slot)
+                    if keep_history:
+                        r.history = self.engine.history(slot)
+                    else:
+                        self.engine.history(slot, count=min(info["samples"], 1))   # results leave the device
+                    r.status = info["status"]
+                    r.done_s = time.perf_counter() - t0
+                    work += float(r.inst.n_voxel) * info["step"]
+                    self.engine.remove(slot)
+                    self.used -= r.fp
+                    done.append(r)
+                    if log:
+                        log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
+        makespan = time.perf_counter() - t0
+        return done, {"makespan_s": makespan, "voxel_steps": work, "launches": self.launches}
+
+    def close(self):
+        self.pool.shutdown(wait=True)
+        self.engine.close()
+
+
+def summarize(done, totals, requests, time_scale=1.0):
+    lat = np.array([r.done_s - r.arrival_s * time_scale for r in done])
+    wait = np.array([r.admit_s - r.arrival_s * time_scale for r in done])
+    span = max(r.arrival_s for r in requests) * time_scale if requests else 0.0
+    offered = sum(r.inst.n_voxel * r.inst.n_steps for r in done) / max(span, 1e-9)
+    return {"requests": len(done), "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "p50_queue_s": float(np.percentile(wait, 50)),
+            "throughput_voxel_steps_s": totals["voxel_steps"] / totals["makespan_s"],
+            "offered_voxel_steps_s": offered, "makespan_s": totals["makespan_s"],
+            "launches": totals["launches"], "arrival_span_s": span,
+            "failed": int(sum(1 for r in done if r.status == _lib.PHS_ERR_NONFINITE))}

@@ -1,0 +1,46 @@
+"""Serving on the GPU: results alone and in the mix are identical; a short
+Poisson run completes every request."""
+import numpy as np
+import pytest
+
+from pyheartsim_b200 import serving
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_requests():
+    reqs = [serving.Request(0, 0.0, 20_000, 30.0, 0, 11_000),
+            serving.Request(1, 0.0, 30_000, 20.0, 1, 12_000),
+            serving.Request(2, 0.0, 25_000, 25.0, 0, 13_000)]
+    return reqs
+
+
+def test_result_alone_equals_result_in_the_mix(cuda_device):
+    alone = {}
+    for r in _small_requests():
+        srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40)
+        done, _ = srv.run([r], keep_history=True)
+        srv.close()
+        alone[r.rid] = done[0].history
+    # all three together, the later ones admitted while the first is running
+    mix = _small_requests()
+    mix[1].arrival_s = 0.05
+    mix[2].arrival_s = 0.10
+    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40, rebalance_every=2)
+    done, totals = srv.run(mix, keep_history=True)
+    srv.close()
+    assert len(done) == 3
+    for r in done:
+        assert r.status == 0
+        assert r.history.shape == alone[r.rid].shape
+        np.testing.assert_array_equal(r.history, alone[r.rid])   # bit-identical
+
+
+def test_short_poisson_run_completes(cuda_device):
+    reqs = serving.poisson_requests(6, rate_per_s=20.0, n_min=20_000, n_max=60_000, dur_ms=(20.0, 60.0), seed=7)
+    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=50)
+    done, totals = srv.run(reqs)
+    srv.close()
+    s = serving.summarize(done, totals, reqs)
+    assert s["requests"] == 6 and s["failed"] == 0
+    assert s["p99_latency_s"] >= s["p50_latency_s"] > 0
