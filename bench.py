@@ -30,6 +30,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
+# DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on a 16-shell, 2.37M-voxel launch at 4.0 Arnoldi steps per
+# solve (profiles/step_kernel_16shells_full.md); scaled to a full launch below.
+STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 363.5
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
 
 
@@ -246,6 +250,7 @@ def run_b200(args):
     value = total_vs / (ms_max / 1e3)
     pk, pk_src = peaks()
     achieved = alg_bytes / launches / (ms / launches / 1e3) / 1e9 if launches else 0.0
+    # achieved is GB/s of algorithmic bytes per launch over the average launch time
     phases = phase_profile(eng, slots, S, stream)
     eng.close()
 
@@ -263,7 +268,9 @@ def run_b200(args):
                        "arnoldi_per_step": float(k_sum.sum() / (K * len(ns)))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
-                         "traffic": None, "kernel": "step_kernel<float,4>",
+                         "traffic": STEP_TRAFFIC_BYTES_PER_VOXEL_STEP * float(ns.sum()) * S,
+                         "traffic_source": "ncu dram bytes per voxel-step (2.37M-voxel capture, k=4.0) x voxels x steps per launch",
+                         "kernel": "step_kernel<float,4>",
                          "bytes_per_voxel_step": alg_bytes / local_vs},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "phases_ms_per_step": phases}

@@ -134,6 +134,10 @@ int64_t phs_engine_launch_count(phs_engine* eng);
 #define PHS_CFG_VARIANT      1
 #define PHS_CFG_CTAS_PER_SM  2
 #define PHS_CFG_PROFILE      3   /* 1: per-instance device phase timers on (small overhead) */
+#define PHS_CFG_TEST_TEAM_OVERCOUNT 4  /* test hook: the first team of the next plan waits for a CTA
+                                          that is never launched; its bounded barrier gives up after
+                                          4 s and advance() returns PHS_ERR_TIMEOUT (the engine is
+                                          then unusable, the CUDA context is not affected)        */
 int phs_engine_config(phs_engine* eng, int key, int64_t value);
 /* Compiled step-kernel variants of a precision: count, and per variant the
  * minimum CTAs per SM it was compiled for and its register count (arrays of at

@@ -32,6 +32,7 @@ EGM_BF16X3 = 1
 CFG_VARIANT = 1
 CFG_CTAS_PER_SM = 2
 CFG_PROFILE = 3
+CFG_TEST_TEAM_OVERCOUNT = 4
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
                  "check", "check_wait", "copy", "step_wait", "steps", "arnoldi_iters", "team_ctas")
 
@@ -184,9 +185,12 @@ def status_string(status):
         return f"status {status}"
 
 
-def check(status, where, allow_warn=False):
-    """Raise PhsError unless ``status`` is OK (or the no-convergence warning when allowed)."""
+def check(status, where, allow_warn=False, allow_nonfinite=False):
+    """Raise PhsError unless ``status`` is OK (or the no-convergence warning /
+    a per-instance non-finite retirement when allowed)."""
     if status == PHS_OK or (allow_warn and status == PHS_WARN_NO_CONVERGE):
+        return status
+    if allow_nonfinite and status == PHS_ERR_NONFINITE:
         return status
     raise PhsError(status, where)
 

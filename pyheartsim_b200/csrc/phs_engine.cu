@@ -1046,6 +1046,7 @@ struct phs_engine {
     bool graphs_ok = true;
     int variant = -1;        // step-kernel variant (-1: default of the precision)
     bool profile = false;    // per-instance phase timers
+    bool test_overcount = false;  // test hook: first team waits for one CTA too many
     int default_cps = 0;     // CTAs per SM when advance() is given 0 (0: occupancy limit)
 };
 
@@ -1359,7 +1360,10 @@ int build_plan(phs_engine* e, int cps) {
         int grid = 0;
         for (size_t i = w0; i < w1; ++i) {
             int p = P[i - w0];
-            for (int r = 0; r < p; ++r) map_all.push_back(make_int4((int)i, r, p, 0));
+            // test hook: the first team expects one CTA that is never launched, so
+            // its first barrier can only end through the bounded wait
+            const int claimed = p + ((e->test_overcount && i == w0) ? 1 : 0);
+            for (int r = 0; r < p; ++r) map_all.push_back(make_int4((int)i, r, claimed, 0));
             grid += p;
         }
         waves.push_back({off, grid});
@@ -1634,6 +1638,10 @@ int phs_engine_config(phs_engine* e, int key, int64_t value) {
         case PHS_CFG_CTAS_PER_SM:
             if (value < 0 || value > 32) return PHS_ERR_BAD_ARG;
             e->default_cps = (int)value;
+            return PHS_OK;
+        case PHS_CFG_TEST_TEAM_OVERCOUNT:
+            e->test_overcount = value != 0;
+            e->dirty = true;
             return PHS_OK;
         case PHS_CFG_PROFILE:
             cudaDeviceSynchronize();

@@ -44,12 +44,14 @@ class BatchedEngine:
         """Advance every unfinished instance by up to ``n_steps`` steps.
 
         ``stream`` is a cudaStream_t handle (int) or a torch.cuda.Stream.
-        Returns the worst instance status (OK or the no-convergence warning)."""
+        Returns the worst instance status: OK, the no-convergence warning, or
+        PHS_ERR_NONFINITE when an instance was retired (the others continue;
+        see :meth:`info`).  Other failures raise."""
         if stream is not None and hasattr(stream, "cuda_stream"):
             stream = stream.cuda_stream
         st = _lib.lib().phs_engine_advance(self._h, int(n_steps), int(ctas_per_sm),
                                            ctypes.c_void_p(stream) if stream else None, 1 if sync else 0)
-        return _lib.check(st, "phs_engine_advance", allow_warn=True)
+        return _lib.check(st, "phs_engine_advance", allow_warn=True, allow_nonfinite=True)
 
     def info(self, slot):
         i = _lib.InstanceInfo()
@@ -82,6 +84,9 @@ class BatchedEngine:
         _lib.check(_lib.lib().phs_instance_read_state(self._h, slot, _lib.vptr(u), _lib.vptr(h),
                                                       _lib.ptr(lat, ctypes.c_int32)), "phs_instance_read_state")
         return u, h, lat
+
+    def config(self, key, value):
+        _lib.check(_lib.lib().phs_engine_config(self._h, int(key), int(value)), "phs_engine_config")
 
     def configure(self, variant=None, ctas_per_sm=None):
         """Select the step-kernel variant and the CTAs per SM used by advance()."""

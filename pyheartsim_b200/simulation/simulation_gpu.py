@@ -27,7 +27,7 @@ from .. import instance as _instance
 
 def compute(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
             dtype=np.float64, fast=False, tol=1e-5, atol=1e-5, restart=None, method='gmres',
-            pacing_duration=None, return_lat=False, return_info=False, max_steps=None):
+            pacing_duration=None, return_lat=False, return_info=False, max_steps=None, maxiter=10000):
     if method != 'gmres':
         raise ValueError(f"Unknown solver method: {method}. Use 'gmres'")
     precision = _lib.PREC_F64 if np.dtype(dtype) == np.float64 else _lib.PREC_F32
@@ -35,7 +35,7 @@ def compute(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_para
         restart = 20 if fast else 50
     inst = _instance.compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters,
                             full_cycles=not fast, tol=tol, atol=atol, restart=restart,
-                            pacing_duration=pacing_duration, max_steps=max_steps)
+                            pacing_duration=pacing_duration, max_steps=max_steps, maxiter=maxiter)
     dt_np = _lib.np_dtype(precision)
     S, n = inst.n_samples, inst.n_voxel
     u_hist = np.zeros((S, n), dtype=dt_np)
