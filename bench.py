@@ -244,7 +244,9 @@ def run_b200(args):
     k_sum = np.array([b["arnoldi_steps"] - a["arnoldi_steps"] for a, b in zip(info0, info1)], dtype=np.float64)
     k_sq = np.array([b["arnoldi_sq"] - a["arnoldi_sq"] for a, b in zip(info0, info1)], dtype=np.float64)
     solves = np.array([b["solves"] - a["solves"] for a, b in zip(info0, info1)], dtype=np.float64)
-    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq) for n, ks, kq in zip(ns, k_sum, k_sq)))
+    iso = [x.cw is not None for x in insts]
+    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, io)
+                          for n, ks, kq, sv, io in zip(ns, k_sum, k_sq, solves, iso)))
     local_vs = float(ns.sum()) * K
     total_vs = local_vs * world
     value = total_vs / (ms_max / 1e3)

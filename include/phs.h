@@ -67,7 +67,8 @@ typedef struct phs_instance_desc {
     int32_t model;            /* PHS_MODEL_MS / PHS_MODEL_AP                              */
     int32_t restart;          /* GMRES restart length m (reference: 50), 1..50            */
     const int32_t* nb6;       /* [n][6] neighbours +x,-x,+y,-y,+z,-z; absent (-1) -> 0 as in the reference */
-    const double* coef6;      /* [n][6] c_n/(4 Delta^2) * P_2d[n,k]  (permanent block: 0)   */
+    const double* coef6;      /* [n][6] c_n/(4 Delta^2) * P_2d[n,k]  (permanent block: 0), or
+                                 NULL when every row is isotropic (cw, mask6 below)         */
     const uint8_t* vflags;    /* [n] PHS_VFLAG_* bits                                       */
     const double* vparams;    /* [n][5] P_2d[:,15:20], or NULL to use params[]              */
     double params[5];         /* MS: tau_open, tau_close, tau_in, tau_out, v_gate;
@@ -86,6 +87,8 @@ typedef struct phs_instance_desc {
     double tol, atol;         /* stop when ||r|| <= max(atol, tol*||b||)                    */
     int32_t maxiter;          /* Arnoldi steps per solve before giving up (reference 10000) */
     int32_t _reserved;
+    const double* cw;         /* [n] isotropic rows: the one non-zero coefficient of row n  */
+    const uint8_t* mask6;     /* [n] isotropic rows: bit k set when coefficient k is cw[n]  */
 } phs_instance_desc;
 
 /* Per-instance progress and solver statistics. */

@@ -74,6 +74,8 @@ class InstanceDesc(ctypes.Structure):
         ("atol", ctypes.c_double),
         ("maxiter", ctypes.c_int32),
         ("_reserved", ctypes.c_int32),
+        ("cw", c_double_p),
+        ("mask6", c_uint8_p),
     ]
 
 

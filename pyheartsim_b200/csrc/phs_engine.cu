@@ -96,7 +96,9 @@ struct InstState {
 template <typename T>
 struct InstDev {
     const int32_t* nb;      // [n*6]
-    const T* coef;          // [n*6]
+    const T* coef;          // [n*6], or nullptr when every row is isotropic (cw, m6)
+    const T* cw;            // [n] common coefficient of row n (isotropic rows)
+    const uint8_t* m6;      // [n] neighbour presence bits of row n (isotropic rows)
     const uint8_t* vflags;  // [n]
     const T* vparams;       // [n*5] or nullptr
     const uint8_t* stim;    // [n_steps]
@@ -308,6 +310,20 @@ __device__ __forceinline__ void load_coef(const double* cf, long long n, double 
     const double2* p = reinterpret_cast<const double2*>(cf + 6 * n);
     double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
     c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y; c[4] = d.x; c[5] = d.y;
+}
+
+// Coefficients of row n: one common value and a presence mask for isotropic
+// rows (D0 = I gives c_n / Delta^2 on every present neighbour), else six values.
+template <typename T>
+__device__ __forceinline__ void row_coef(const T* coef, const T* cw, const uint8_t* m6, long long n, T (&c)[6]) {
+    if (cw) {
+        const T w = cw[n];
+        const unsigned mk = __ldg(m6 + n);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) c[k] = ((mk >> k) & 1u) ? w : T(0);
+    } else {
+        load_coef(coef, n, c);
+    }
 }
 
 // Matrix-free row of L applied to `vec` at voxel n (coefficients already loaded);
@@ -666,7 +682,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     int32_t q[6];
                     T c[6];
                     load_nb(I.nb, n, q);
-                    load_coef(I.coef, n, c);
+                    row_coef(I.coef, I.cw, I.m6, n, c);
                     T lap = T(0);
                     if (!rz) {
                         T uq[6], hq[6];
@@ -741,7 +757,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                                 int32_t q[6];
                                 T c[6];
                                 load_nb(I.nb, n, q);
-                                load_coef(I.coef, n, c);
+                                row_coef(I.coef, I.cw, I.m6, n, c);
                                 const T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
                                 const T w = sj * (vj - I.half_dt * lap);
                                 Vn[n] = w;
@@ -859,7 +875,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             int32_t q[6];
                             T c[6];
                             load_nb(I.nb, n, q);
-                            load_coef(I.coef, n, c);
+                            row_coef(I.coef, I.cw, I.m6, n, c);
                             const T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
                             const T ax = xv - I.half_dt * lap;
                             const T r = I.b[n] - ax;
@@ -988,6 +1004,8 @@ struct InstHost {
     int m = 0;
     void* nb = nullptr;
     void* coef = nullptr;
+    void* cw = nullptr;
+    void* m6 = nullptr;
     void* vflags = nullptr;
     void* vparams = nullptr;
     void* stim = nullptr;
@@ -1015,7 +1033,7 @@ struct InstHost {
 };
 
 void free_inst(InstHost& h) {
-    void* ptrs[] = {h.nb, h.coef, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
+    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
                     h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1090,7 +1108,8 @@ int validate_desc(const phs_instance_desc* d) {
     if (!d || d->n_voxel <= 0 || d->n_voxel > (1ll << 31) - 1) return PHS_ERR_BAD_ARG;
     if (d->model != PHS_MODEL_MS && d->model != PHS_MODEL_AP) return PHS_ERR_BAD_ARG;
     if (d->restart < 1 || d->restart > kMaxRestart) return PHS_ERR_BAD_ARG;
-    if (!d->nb6 || !d->coef6 || !d->vflags) return PHS_ERR_BAD_ARG;
+    if (!d->nb6 || !d->vflags) return PHS_ERR_BAD_ARG;
+    if (!d->coef6 && !(d->cw && d->mask6)) return PHS_ERR_BAD_ARG;
     if (d->n_steps < 0 || (d->n_steps > 0 && !d->stim)) return PHS_ERR_BAD_ARG;
     if (d->n_samples < 0 || d->sample_stride < 0 || d->maxiter < 1) return PHS_ERR_BAD_ARG;
     if (!(d->dt > 0.0)) return PHS_ERR_BAD_ARG;
@@ -1098,8 +1117,11 @@ int validate_desc(const phs_instance_desc* d) {
     for (long long i = 0; i < 6 * n; ++i) {
         int32_t q = d->nb6[i];
         if (q < 0 || q >= n) return PHS_ERR_BAD_TABLE;
-        if (!std::isfinite(d->coef6[i])) return PHS_ERR_BAD_TABLE;
+        if (d->coef6 && !std::isfinite(d->coef6[i])) return PHS_ERR_BAD_TABLE;
     }
+    if (d->cw)
+        for (long long i = 0; i < n; ++i)
+            if (!std::isfinite(d->cw[i]) || (d->mask6[i] & 0xC0u)) return PHS_ERR_BAD_TABLE;
     return PHS_OK;
 }
 
@@ -1124,7 +1146,13 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     } while (0)
     PHS_ALLOC(h.nb, n * 6 * sizeof(int32_t));
     if (cudaMemcpy(h.nb, d->nb6, n * 6 * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
-    if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6)) != PHS_OK) return fail(rc);
+    if (d->cw) {
+        if ((rc = upload_converted<T>(&h.cw, d->cw, (long long)n)) != PHS_OK) return fail(rc);
+        PHS_ALLOC(h.m6, n);
+        if (cudaMemcpy(h.m6, d->mask6, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
+    } else {
+        if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6)) != PHS_OK) return fail(rc);
+    }
     PHS_ALLOC(h.vflags, n);
     if (cudaMemcpy(h.vflags, d->vflags, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
     if (d->vparams) {
@@ -1196,6 +1224,8 @@ InstDev<T> make_dev(const InstHost& h) {
     InstDev<T> I{};
     I.nb = (const int32_t*)h.nb;
     I.coef = (const T*)h.coef;
+    I.cw = (const T*)h.cw;
+    I.m6 = (const uint8_t*)h.m6;
     I.vflags = (const uint8_t*)h.vflags;
     I.vparams = (const T*)h.vparams;
     I.stim = (const uint8_t*)h.stim;

@@ -73,7 +73,10 @@ class BatchedEngine:
         h = np.empty((count, inst.n_voxel), dtype=dt) if with_h else None
         _lib.check(_lib.lib().phs_instance_read_history(self._h, slot, s0, count, _lib.vptr(u), _lib.vptr(h)),
                    "phs_instance_read_history")
-        return (u, h) if with_h else u
+        u = inst.to_caller(u)
+        if with_h:
+            return u, inst.to_caller(h)
+        return u
 
     def state(self, slot):
         inst = self._inst[slot]
@@ -83,7 +86,7 @@ class BatchedEngine:
         lat = np.empty(inst.n_voxel, dtype=np.int32)
         _lib.check(_lib.lib().phs_instance_read_state(self._h, slot, _lib.vptr(u), _lib.vptr(h),
                                                       _lib.ptr(lat, ctypes.c_int32)), "phs_instance_read_state")
-        return u, h, lat
+        return inst.to_caller(u), inst.to_caller(h), inst.to_caller(lat)
 
     def config(self, key, value):
         _lib.check(_lib.lib().phs_engine_config(self._h, int(key), int(value)), "phs_engine_config")

@@ -21,6 +21,43 @@ from . import _lib
 from .simulation import pacing
 
 
+def _spread_bits(x):
+    """Spread the low 21 bits of x to every third bit (Morton interleave)."""
+    x = x.astype(np.uint64) & np.uint64(0x1fffff)
+    for sh, m in ((32, 0x1f00000000ffff), (16, 0x1f0000ff0000ff), (8, 0x100f00f00f00f00f),
+                  (4, 0x10c30c30c30c30c3), (2, 0x1249249249249249)):
+        x = (x | (x << np.uint64(sh))) & np.uint64(m)
+    return x
+
+
+def locality_order(geometry_data, n, kind="rows"):
+    """Device order of the voxels, from the lattice coordinates ``voxel / Delta``.
+
+    ``rows`` (default): lexicographic (z, y, x) with x fastest, so rows along x
+    are contiguous; inside a tile of consecutive voxels the +-x and most +-y
+    neighbours are present, and the neighbours outside the tile are the +-z ones
+    for whole warps at a time (the stencil's recomputation stays uniform across
+    a warp).  ``morton``: Z-curve order (fewer neighbours outside a tile, but
+    they are scattered across the lanes of a warp).
+    Returns ``order`` (device index -> caller index), or None when the geometry
+    carries no coordinates."""
+    vox = geometry_data.get('voxel') if hasattr(geometry_data, 'get') else None
+    if vox is None:
+        return None
+    vox = np.asarray(vox, dtype=np.float64)
+    if vox.shape != (n, 3):
+        return None
+    ijk = np.rint(vox / float(geometry_data['Delta'])).astype(np.int64)
+    ijk -= ijk.min(axis=0)
+    if kind == "rows":
+        return np.lexsort((ijk[:, 0], ijk[:, 1], ijk[:, 2]))
+    if ijk.max() >= (1 << 21):
+        return None
+    code = _spread_bits(ijk[:, 0]) | (_spread_bits(ijk[:, 1]) << np.uint64(1)) | \
+        (_spread_bits(ijk[:, 2]) << np.uint64(2))
+    return np.argsort(code, kind='stable')
+
+
 class CompiledInstance:
     """Host arrays + scalars of one instance, and the ctypes descriptor over them."""
 
@@ -35,7 +72,10 @@ class CompiledInstance:
         d.model = self.model
         d.restart = self.restart
         d.nb6 = _lib.ptr(self.nb6, _lib.ctypes.c_int32)
-        d.coef6 = _lib.ptr(self.coef6, _lib.ctypes.c_double)
+        iso = getattr(self, "cw", None) is not None
+        d.coef6 = None if iso else _lib.ptr(self.coef6, _lib.ctypes.c_double)
+        d.cw = _lib.ptr(self.cw, _lib.ctypes.c_double) if iso else None
+        d.mask6 = _lib.ptr(self.mask6, _lib.ctypes.c_uint8) if iso else None
         d.vflags = _lib.ptr(self.vflags, _lib.ctypes.c_uint8)
         d.vparams = _lib.ptr(self.vparams, _lib.ctypes.c_double) if self.vparams is not None else None
         for i in range(5):
@@ -56,6 +96,10 @@ class CompiledInstance:
         d.maxiter = self.maxiter
         self._desc = d
         return d
+
+    def to_caller(self, a):
+        """Map device-ordered voxel data (last axis) back to the caller's order."""
+        return a if self.inv is None else a[..., self.inv]
 
     def sample_times(self, n_saved):
         """physical_time of the first ``n_saved`` samples: the sample taken after
@@ -94,12 +138,15 @@ def tblock_steps(n_steps, dt):
 
 def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
                      full_cycles=True, tol=1e-5, atol=1e-5, restart=50, maxiter=10000,
-                     pacing_duration=None, save_h=True, max_steps=None):
+                     pacing_duration=None, save_h=True, max_steps=None, reorder="rows"):
     """Build a :class:`CompiledInstance` with the reference's semantics.
 
     ``full_cycles=True`` keeps CuPy's GMRES(restart) behaviour (the plain
     drop-in); ``False`` stops each solve as soon as the Givens residual
-    estimate meets the same tolerance.
+    estimate meets the same tolerance.  With ``reorder`` ("rows" by default,
+    "morton", or False) and voxel coordinates in ``geometry_data``, voxels are
+    stored in that order on the device; results are mapped back with
+    :meth:`CompiledInstance.to_caller`.
     """
     n = int(n_voxel)
     P = np.asarray(P_2d, dtype=np.float64)
@@ -147,6 +194,26 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
     uniform = bool(np.all(mp == mp[0:1]))
     params = mp[0].copy() if n else np.zeros(5)
     vparams = None if uniform else np.ascontiguousarray(mp)
+    # isotropic rows: every non-zero coefficient of a row is the same value
+    nz = coef6 != 0
+    cw = np.where(nz.any(axis=1), coef6[np.arange(n), nz.argmax(axis=1)], 0.0)
+    mask6 = (nz * (1 << np.arange(6))).sum(axis=1).astype(np.uint8)
+    if not np.array_equal(coef6, cw[:, None] * nz):
+        cw = mask6 = None
+    order = locality_order(geometry_data, n, reorder) if reorder else None
+    if order is not None and np.array_equal(order, np.arange(n)):
+        order = None
+    inv = None
+    if order is not None:
+        inv = np.empty(n, dtype=np.int64)
+        inv[order] = np.arange(n)
+        nb6 = inv[nb6[order]]
+        coef6 = coef6[order]
+        vflags = vflags[order]
+        if cw is not None:
+            cw, mask6 = cw[order], mask6[order]
+        if vparams is not None:
+            vparams = np.ascontiguousarray(vparams[order])
     u0, h0 = (0.0, 1.0) if model == 0 else (0.0, 0.0)
     return CompiledInstance(
         n_voxel=n, model=model, restart=int(min(restart, 50)), nb6=np.ascontiguousarray(nb6, dtype=np.int32),
@@ -154,4 +221,5 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         j_stim=float(jmag), n_steps=int(n_steps), stim=np.ascontiguousarray(stim, dtype=np.uint8),
         tblock_steps=int(tb), sample_stride=int(stride), n_samples=int(n_samples), save_h=int(bool(save_h)),
         full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol), atol=float(atol),
-        maxiter=int(maxiter), time_scale=ts, Delta=Delta)
+        maxiter=int(maxiter), time_scale=ts, Delta=Delta, order=order, inv=inv,
+        cw=None if cw is None else np.ascontiguousarray(cw), mask6=None if mask6 is None else np.ascontiguousarray(mask6))

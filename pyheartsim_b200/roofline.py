@@ -1,50 +1,43 @@
 """Algorithmic DRAM bytes of the step kernel, per voxel-step.
 
-The model counts every array the kernel must stream once per phase (s = bytes
-per stored value: 4 for FP32, 8 for FP64; neighbour values are assumed to hit
-in cache, as their owners stream them in the same phase):
+Counts every array the kernel must stream once per phase; s = bytes per stored
+value (4 FP32, 8 FP64), cb = coefficient bytes per row (5 for isotropic rows:
+one value + a presence byte; 6 s otherwise).  Neighbour values read by the
+stencil are assumed to hit in cache (their owners stream them in the same
+phase).
 
-  RHS phase  read u, h, flags, nb[6] (int32), coef[6]; write x, h', b, V0
-             = 2s + 1 + 24 + 6s + 4s
-  phase A_j  read V_j, nb, coef, V_0..V_{j-1}; write w           = 2s + 24 + 6s + js
-  phase C_j  read w, V_0..V_j; write V_{j+1}                     = (j+3)s
-  update     read x, V_0..V_{k-1}; write u (or x)                = (k+2)s
-  check      read x, nb, coef, b; write V0, u (full cycles only) = 5s + 24 + 6s
+  RHS        read u, h, flags, nb[6] (int32), coefficients; write x, h', b, V0
+             = 6 s + 25 + cb
+  phase A_j  read V_j, nb, coefficients, V_0..V_{j-1}; write w  = (j + 2) s + 24 + cb
+  phase C_j  read w, V_0..V_j; write V_{j+1}                     = (j + 3) s
+  update     read x, V_0..V_{k-1}; write u                       = (k + 2) s
+  copy       (a solve that needs no iteration) read x, write u  = 2 s
 
 A solve with k Arnoldi steps therefore costs
-  B(k) = RHS + update + sum_{j<k} (A_j + C_j)
-       = (13s + 25) + (k+2)s + k(11s + 24) + s k(k-1)
-For FP32 this is 81 + 68 k + 4 k^2 bytes (k = 0 when the initial residual
-already meets the tolerance).
+  B(k) = RHS + (k + 2) s + k (5 s + 24 + cb) + s k (k - 1),
+e.g. 81 + 68 k + 4 k^2 bytes in FP32 with six stored coefficients, and
+62 + 49 k + 4 k^2 with isotropic rows.
 """
 
 
-def bytes_rhs(s):
-    return 2 * s + 1 + 24 + 6 * s + 4 * s
+def coef_bytes(s, iso):
+    return (s + 1) if iso else 6 * s
 
 
-def bytes_iter_sum(s, k_sum, k_sq_sum):
-    """sum over solves of sum_{j<k}(A_j + C_j) = sum_k [k(11s+24) + s k(k-1)]."""
-    return (11 * s + 24) * k_sum + s * (k_sq_sum - k_sum)
+def bytes_rhs(s, cb):
+    return 6 * s + 25 + cb
 
 
-def bytes_update(s, k_sum, solves):
-    return (2 * s) * solves + s * k_sum
-
-
-def bytes_check(s):
-    return 5 * s + 24 + 6 * s
-
-
-def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, checks=0):
+def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True):
     """Total algorithmic bytes of ``steps`` steps of an instance with ``voxels``
     voxels whose solves took ``k_sum`` Arnoldi steps in total (``k_sq_sum`` =
     sum of squares).  Steps that needed no iteration still run the RHS phase
-    and the final copy (2s)."""
-    per_voxel = (steps * (bytes_rhs(s) + 2 * s) + bytes_iter_sum(s, k_sum, k_sq_sum) + s * k_sum
-                 + checks * bytes_check(s))
+    and the final copy (2 s)."""
+    cb = coef_bytes(s, iso)
+    per_voxel = (steps * (bytes_rhs(s, cb) + 2 * s) + (5 * s + 24 + cb) * k_sum + s * (k_sq_sum - k_sum)
+                 + s * k_sum)
     return voxels * per_voxel
 
 
-def per_voxel_step(s, k):
-    return bytes_rhs(s) + 2 * s + bytes_iter_sum(s, k, k * k) + s * k
+def per_voxel_step(s, k, iso=True):
+    return algorithmic_bytes(s, 1, 1, k, k * k, iso=iso)

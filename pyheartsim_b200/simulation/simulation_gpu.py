@@ -54,9 +54,9 @@ def compute(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_para
     k = int(n_saved.value)
     t = inst.sample_times(k)
     t = t.astype(dt_np)
-    out = (u_hist[:k], h_hist[:k], t)
+    out = (inst.to_caller(u_hist[:k]), inst.to_caller(h_hist[:k]), t)
     if return_lat:
-        out = out + (lat,)
+        out = out + (inst.to_caller(lat),)
     if return_info:
         out = out + ({"steps": int(info.step), "arnoldi_steps": int(info.arnoldi_steps),
                       "solves": int(info.solves), "max_arnoldi": int(info.max_arnoldi),

@@ -47,7 +47,7 @@ def test_step_counts_match_reference(t_final, dt, model):
 @pytest.mark.parametrize("name", golden_cases.names())
 def test_matrix_free_operator_equals_reference_csr(name):
     c = golden_cases.load(name)
-    inst = instance.compile_instance(c["n"], c["P_2d"], c["geom"], c["sp"], c["ap"])
+    inst = instance.compile_instance(c["n"], c["P_2d"], c["geom"], c["sp"], c["ap"], reorder=False)
     P = np.array(c["P_2d"], dtype=np.float64)
     nf = np.asarray(c["ap"]["node_flag"])
     P[nf == 4, 20] = 0.0
@@ -123,3 +123,24 @@ def test_shell_generator_is_seeded_and_sized():
     assert 60_000 < a.shape[0] < 130_000
     nb = synthetic.lattice_neighbors(a) if hasattr(synthetic, "lattice_neighbors") else None
     assert nb is not None and nb.shape == (a.shape[0], 18)
+
+
+def test_reorder_preserves_the_operator():
+    from pyheartsim_b200 import synthetic
+    ijk = synthetic.shell((6.0, 5.0, 4.0), 0.4, 2, 1, 1.5, 0)
+    s1 = np.arange(5)
+    n, P, geom, sp, ap = synthetic.make_case(ijk, 0.4, 0, 0.05, 5.0, s1, flag=4)
+    a = instance.compile_instance(n, P, geom, sp, ap, reorder=False)
+    b = instance.compile_instance(n, P, geom, sp, ap, reorder="morton")
+    assert b.order is not None and not np.array_equal(b.order, np.arange(n))
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal(n)
+    lap_a = (a.coef6 * (u[a.nb6] - u[:, None])).sum(axis=1)
+    ub = u[b.order]                                       # device order
+    lap_b = (b.coef6 * (ub[b.nb6] - ub[:, None])).sum(axis=1)
+    np.testing.assert_allclose(b.to_caller(lap_b), lap_a, rtol=1e-13, atol=1e-13)
+    np.testing.assert_array_equal(b.to_caller(b.vflags), a.vflags)
+    # tiles of 1024 device-ordered voxels keep most neighbours inside
+    tile = np.arange(n) // 1024
+    out = (b.coef6 != 0) & (b.nb6 // 1024 != tile[:, None])
+    assert out.sum() / n < 1.0
