@@ -245,8 +245,9 @@ def run_b200(args):
     k_sq = np.array([b["arnoldi_sq"] - a["arnoldi_sq"] for a, b in zip(info0, info1)], dtype=np.float64)
     solves = np.array([b["solves"] - a["solves"] for a, b in zip(info0, info1)], dtype=np.float64)
     iso = [x.cw is not None for x in insts]
-    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, io)
-                          for n, ks, kq, sv, io in zip(ns, k_sum, k_sq, solves, iso)))
+    gs = [bool(x.guess) for x in insts]
+    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, io, g)
+                          for n, ks, kq, sv, io, g in zip(ns, k_sum, k_sq, solves, iso, gs)))
     local_vs = float(ns.sum()) * K
     total_vs = local_vs * world
     value = total_vs / (ms_max / 1e3)

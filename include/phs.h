@@ -86,7 +86,9 @@ typedef struct phs_instance_desc {
     double u0, h0;            /* initial state (MS: 0,1; AP: 0,0)                           */
     double tol, atol;         /* stop when ||r|| <= max(atol, tol*||b||)                    */
     int32_t maxiter;          /* Arnoldi steps per solve before giving up (reference 10000) */
-    int32_t _reserved;
+    int32_t guess;            /* 0: start each solve from u* (the reference's x0); 1: from u*
+                                 plus the previous step's diffusion increment (same stopping
+                                 test, fewer iterations)                                    */
     const double* cw;         /* [n] isotropic rows: the one non-zero coefficient of row n  */
     const uint8_t* mask6;     /* [n] isotropic rows: bit k set when coefficient k is cw[n]  */
 } phs_instance_desc;

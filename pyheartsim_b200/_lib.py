@@ -73,7 +73,7 @@ class InstanceDesc(ctypes.Structure):
         ("tol", ctypes.c_double),
         ("atol", ctypes.c_double),
         ("maxiter", ctypes.c_int32),
-        ("_reserved", ctypes.c_int32),
+        ("guess", ctypes.c_int32),
         ("cw", c_double_p),
         ("mask6", c_uint8_p),
     ]

@@ -108,6 +108,7 @@ struct InstDev {
     T* x;
     T* b;
     T* V;                   // [(m+1)*n]
+    T* dx;                  // [n] last diffusion increment (extrapolated initial guess), or nullptr
     T* hist_u;              // [S*n]
     T* hist_h;              // [S*n] or nullptr
     int32_t* lat;           // [n]
@@ -665,7 +666,6 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
                     T us, hs;
                     rk4(I.model, un, hn, J, p, I.dt, us, hs);
-                    I.x[n] = us;
                     hout[n] = hs;
                     us_reg[v] = us;
                     ustar_tile[v * kThreads + threadIdx.x] = us;
@@ -712,9 +712,18 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             lap += c[k] * (usq - us);
                         }
                     }
+                    // initial guess: u* (the reference's x0), or u* plus the previous
+                    // step's diffusion increment when dx is kept
+                    T dp = T(0), lapd = T(0);
+                    if (I.dx) {
+                        dp = I.dx[n];
+                        if (!rz) lapd = lap_row(I.dx, dp, q, c);
+                    }
+                    const T x0 = us + dp;
                     const T bn = us + I.half_dt * lap;
-                    const T ax = us - I.half_dt * lap;
+                    const T ax = x0 - I.half_dt * (lap + lapd);
                     const T rn = bn - ax;
+                    I.x[n] = x0;
                     I.b[n] = bn;
                     Vb[n] = rn;
                     ab += (double)bn * (double)bn;
@@ -844,19 +853,25 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 load_shc(k);
                 const bool final = (act == ACT_UPDATE_FINAL);
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
-                    double acc[VPT];
+                    double acc[VPT], x_in[VPT];
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
                         const long long n = voxel(tile, v);
                         acc[v] = (n < N) ? (double)I.x[n] : 0.0;
+                        x_in[v] = acc[v];
                     }
                     axpy_basis(tile, k, shc, acc);
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
                         const long long n = voxel(tile, v);
                         if (n < N) {
-                            if (final) I.u[n] = (T)acc[v];
-                            else I.x[n] = (T)acc[v];
+                            if (final) {
+                                I.u[n] = (T)acc[v];
+                                // increment u_next - u* for the next step's initial guess
+                                if (I.dx) I.dx[n] = (T)((double)I.dx[n] + (acc[v] - x_in[v]));
+                            } else {
+                                I.x[n] = (T)acc[v];
+                            }
                         }
                     }
                 }
@@ -1015,6 +1030,7 @@ struct InstHost {
     void* x = nullptr;
     void* b = nullptr;
     void* V = nullptr;
+    void* dx = nullptr;
     void* hist_u = nullptr;
     void* hist_h = nullptr;
     int32_t* lat = nullptr;
@@ -1033,7 +1049,7 @@ struct InstHost {
 };
 
 void free_inst(InstHost& h) {
-    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
+    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
                     h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1171,6 +1187,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     PHS_ALLOC(h.x, n * sizeof(T));
     PHS_ALLOC(h.b, n * sizeof(T));
     PHS_ALLOC(h.V, n * (size_t)(h.m + 1) * sizeof(T));
+    if (d->guess) PHS_ALLOC(h.dx, n * sizeof(T));
     const size_t S = (size_t)std::max(d->n_samples, 1);
     PHS_ALLOC(h.hist_u, S * n * sizeof(T));
     if (d->save_h) PHS_ALLOC(h.hist_h, S * n * sizeof(T));
@@ -1187,6 +1204,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     fill_dev<T>((T*)h.x, (long long)n, (T)0, 0);
     fill_dev<T>((T*)h.b, (long long)n, (T)0, 0);
     cudaMemset(h.V, 0, n * (size_t)(h.m + 1) * sizeof(T));
+    if (h.dx) cudaMemset(h.dx, 0, n * sizeof(T));
     cudaMemset(h.hist_u, 0, S * n * sizeof(T));
     if (h.hist_h) cudaMemset(h.hist_h, 0, S * n * sizeof(T));
     cudaMemset(h.lat, 0xff, n * sizeof(int32_t));
@@ -1235,6 +1253,7 @@ InstDev<T> make_dev(const InstHost& h) {
     I.x = (T*)h.x;
     I.b = (T*)h.b;
     I.V = (T*)h.V;
+    I.dx = (T*)h.dx;
     I.hist_u = (T*)h.hist_u;
     I.hist_h = (T*)h.hist_h;
     I.lat = h.lat;

@@ -94,6 +94,7 @@ class CompiledInstance:
         d.tol = self.tol
         d.atol = self.atol
         d.maxiter = self.maxiter
+        d.guess = int(getattr(self, "guess", 0))
         self._desc = d
         return d
 
@@ -138,7 +139,7 @@ def tblock_steps(n_steps, dt):
 
 def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
                      full_cycles=True, tol=1e-5, atol=1e-5, restart=50, maxiter=10000,
-                     pacing_duration=None, save_h=True, max_steps=None, reorder="rows"):
+                     pacing_duration=None, save_h=True, max_steps=None, reorder="rows", guess=None):
     """Build a :class:`CompiledInstance` with the reference's semantics.
 
     ``full_cycles=True`` keeps CuPy's GMRES(restart) behaviour (the plain
@@ -146,7 +147,9 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
     estimate meets the same tolerance.  With ``reorder`` ("rows" by default,
     "morton", or False) and voxel coordinates in ``geometry_data``, voxels are
     stored in that order on the device; results are mapped back with
-    :meth:`CompiledInstance.to_caller`.
+    :meth:`CompiledInstance.to_caller`.  ``guess`` (default: on for the
+    early-exit form, off for the plain form) starts each solve from u* plus the
+    previous step's diffusion increment instead of u*.
     """
     n = int(n_voxel)
     P = np.asarray(P_2d, dtype=np.float64)
@@ -222,4 +225,5 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         tblock_steps=int(tb), sample_stride=int(stride), n_samples=int(n_samples), save_h=int(bool(save_h)),
         full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol), atol=float(atol),
         maxiter=int(maxiter), time_scale=ts, Delta=Delta, order=order, inv=inv,
+        guess=int((not full_cycles) if guess is None else bool(guess)),
         cw=None if cw is None else np.ascontiguousarray(cw), mask6=None if mask6 is None else np.ascontiguousarray(mask6))

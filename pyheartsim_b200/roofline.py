@@ -12,6 +12,7 @@ phase).
   phase C_j  read w, V_0..V_j; write V_{j+1}                     = (j + 3) s
   update     read x, V_0..V_{k-1}; write u                       = (k + 2) s
   copy       (a solve that needs no iteration) read x, write u  = 2 s
+  guess      (extrapolated initial guess) + s per step, + 2 s per iterated solve
 
 A solve with k Arnoldi steps therefore costs
   B(k) = RHS + (k + 2) s + k (5 s + 24 + cb) + s k (k - 1),
@@ -28,7 +29,7 @@ def bytes_rhs(s, cb):
     return 6 * s + 25 + cb
 
 
-def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True):
+def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False):
     """Total algorithmic bytes of ``steps`` steps of an instance with ``voxels``
     voxels whose solves took ``k_sum`` Arnoldi steps in total (``k_sq_sum`` =
     sum of squares).  Steps that needed no iteration still run the RHS phase
@@ -36,6 +37,8 @@ def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True):
     cb = coef_bytes(s, iso)
     per_voxel = (steps * (bytes_rhs(s, cb) + 2 * s) + (5 * s + 24 + cb) * k_sum + s * (k_sq_sum - k_sum)
                  + s * k_sum)
+    if guess:     # read the increment in the RHS phase; read and rewrite it in the final update
+        per_voxel += steps * s + 2 * s * (solves or 0)
     return voxels * per_voxel
 
 
