@@ -648,32 +648,65 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         const T* hin = hbuf ? I.h1 : I.h0;
         T* hout = hbuf ? I.h0 : I.h1;
 
-        // ================= RHS phase: fused RK4 + b + r0.  The tile's own u* stay
-        // in shared memory; only neighbours outside the tile are recomputed.
+        // ================= RHS phase: fused RK4 + b + r0.  The tile's own u* stay in
+        // shared memory.  The +-z neighbours (outside the tile in row order) get their
+        // RK4 in the same pass as the voxel's own, as independent chains; any other
+        // neighbour outside the tile is recomputed in the rare slow path.
         for (int tile = rank; tile < I.n_tiles; tile += P) {
             const long long base = (long long)tile * TILE;
-            T us_reg[VPT];
-#pragma unroll
+            T us_reg[VPT], z4[VPT], z5[VPT];
+            unsigned zfar = 0u;
+#pragma unroll 2
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
                 us_reg[v] = T(0);
+                z4[v] = T(0);
+                z5[v] = T(0);
                 if (n < N) {
                     const T un = I.u[n], hn = hin[n];
                     const uint8_t f = __ldg(I.vflags + n);
+                    const bool rz = tb && (f & PHS_VFLAG_TBLOCK);
+                    const int2 qz = __ldg(reinterpret_cast<const int2*>(I.nb + 6 * n + 4));
+                    bool f4 = false, f5 = false;
+                    if (!rz) {
+                        if (I.cw) {
+                            const unsigned mk = __ldg(I.m6 + n);
+                            f4 = (mk & 16u) != 0u;
+                            f5 = (mk & 32u) != 0u;
+                        } else {
+                            f4 = I.coef[6 * n + 4] != T(0);
+                            f5 = I.coef[6 * n + 5] != T(0);
+                        }
+                        f4 = f4 && ((long long)qz.x - base < 0 || (long long)qz.x - base >= TILE);
+                        f5 = f5 && ((long long)qz.y - base < 0 || (long long)qz.y - base >= TILE);
+                    }
+                    const long long q4 = f4 ? qz.x : n, q5 = f5 ? qz.y : n;
+                    const T u4 = I.u[q4], h4 = hin[q4], u5 = I.u[q5], h5 = hin[q5];
+                    const uint8_t fl4 = __ldg(I.vflags + q4), fl5 = __ldg(I.vflags + q5);
                     sample_voxel(n, un, hn, step - 1);
-                    T p[5];
+                    T p[5], p4[5], p5[5];
                     params_of(n, p);
+                    params_of(q4, p4);
+                    params_of(q5, p5);
                     const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
-                    T us, hs;
+                    const T J4 = (fl4 & stim_bits & 3u) ? I.jmag : T(0);
+                    const T J5 = (fl5 & stim_bits & 3u) ? I.jmag : T(0);
+                    T us, hs, us4, hs4, us5, hs5;
                     rk4(I.model, un, hn, J, p, I.dt, us, hs);
+                    rk4(I.model, u4, h4, J4, p4, I.dt, us4, hs4);
+                    rk4(I.model, u5, h5, J5, p5, I.dt, us5, hs5);
                     hout[n] = hs;
                     us_reg[v] = us;
+                    z4[v] = us4;
+                    z5[v] = us5;
+                    zfar |= (f4 ? 1u : 0u) << (2 * v);
+                    zfar |= (f5 ? 2u : 0u) << (2 * v);
                     ustar_tile[v * kThreads + threadIdx.x] = us;
                 }
             }
             __syncthreads();
             double ab = 0.0, ar = 0.0;
-#pragma unroll 1
+#pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
                 if (n < N) {
@@ -685,29 +718,24 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     row_coef(I.coef, I.cw, I.m6, n, c);
                     T lap = T(0);
                     if (!rz) {
-                        T uq[6], hq[6];
-                        uint8_t fq[6];
-                        bool far[6];
 #pragma unroll
                         for (int k = 0; k < 6; ++k) {
-                            const long long off = (long long)q[k] - base;
-                            far[k] = (c[k] != T(0)) && (off < 0 || off >= TILE);
-                            uq[k] = far[k] ? I.u[q[k]] : T(0);
-                            hq[k] = far[k] ? hin[q[k]] : T(0);
-                            fq[k] = far[k] ? __ldg(I.vflags + q[k]) : (uint8_t)0;
-                        }
-#pragma unroll 1
-                        for (int k = 0; k < 6; ++k) {
                             if (c[k] == T(0)) continue;
+                            const long long off = (long long)q[k] - base;
                             T usq;
-                            if (far[k]) {
+                            if (off >= 0 && off < TILE) {
+                                usq = ustar_tile[off];
+                            } else if (k == 4 && (zfar >> (2 * v) & 1u)) {
+                                usq = z4[v];
+                            } else if (k == 5 && (zfar >> (2 * v) & 2u)) {
+                                usq = z5[v];
+                            } else {
+                                // slow path: a +-x / +-y neighbour outside the tile
                                 T pq[5];
                                 params_of(q[k], pq);
-                                const T Jq = (fq[k] & stim_bits & 3u) ? I.jmag : T(0);
+                                const T Jq = (__ldg(I.vflags + q[k]) & stim_bits & 3u) ? I.jmag : T(0);
                                 T hsq;
-                                rk4(I.model, uq[k], hq[k], Jq, pq, I.dt, usq, hsq);
-                            } else {
-                                usq = ustar_tile[q[k] - base];
+                                rk4(I.model, I.u[q[k]], hin[q[k]], Jq, pq, I.dt, usq, hsq);
                             }
                             lap += c[k] * (usq - us);
                         }
