@@ -91,6 +91,13 @@ typedef struct phs_instance_desc {
                                  test, fewer iterations)                                    */
     const double* cw;         /* [n] isotropic rows: the one non-zero coefficient of row n  */
     const uint8_t* mask6;     /* [n] isotropic rows: bit k set when coefficient k is cw[n]  */
+    /* Anisotropic tensors (D0 != I).  The face cross terms P_2d[:,6..8] of
+     * simulation/simulation_gpu.py:172-197 are folded into coef6 (+ on the + side,
+     * - on the - side); the edge cross terms P_2d[:,9..14] of :199-217 are six
+     * antisymmetric pairs per row: (L u)_n += coef_edge[n][p] * (u[a] - u[b]) with
+     * a = nb_edge[n][2p], b = nb_edge[n][2p+1].  Both NULL for D0 = I.          */
+    const int32_t* nb_edge;   /* [n][12] edge neighbours (a0,b0,...,a5,b5), absent -> 0     */
+    const double* coef_edge;  /* [n][6]  c_n/(4 Delta^2) * P_2d[n,9+p]                      */
 } phs_instance_desc;
 
 /* Per-instance progress and solver statistics. */

@@ -76,6 +76,8 @@ class InstanceDesc(ctypes.Structure):
         ("guess", ctypes.c_int32),
         ("cw", c_double_p),
         ("mask6", c_uint8_p),
+        ("nb_edge", c_int32_p),
+        ("coef_edge", c_double_p),
     ]
 
 

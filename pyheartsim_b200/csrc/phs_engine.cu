@@ -99,6 +99,8 @@ struct InstDev {
     const T* coef;          // [n*6], or nullptr when every row is isotropic (cw, m6)
     const T* cw;            // [n] common coefficient of row n (isotropic rows)
     const uint8_t* m6;      // [n] neighbour presence bits of row n (isotropic rows)
+    const int32_t* enb;     // [n*12] edge pairs (a0,b0,...,a5,b5) of anisotropic rows, or nullptr
+    const T* ecf;           // [n*6] edge pair coefficients, or nullptr (D0 = I)
     const uint8_t* vflags;  // [n]
     const T* vparams;       // [n*5] or nullptr
     const uint8_t* stim;    // [n_steps]
@@ -337,6 +339,27 @@ __device__ __forceinline__ T lap_row(const T* vec, T vn, const int32_t (&q)[6], 
     T acc = T(0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc += c[k] * (g[k] - vn);
+    return acc;
+}
+
+// Edge cross terms of an anisotropic row n (simulation/simulation_gpu.py:199-217):
+// six antisymmetric pairs ecf[p] * (vec[a_p] - vec[b_p]); all gathers first.
+template <typename T>
+__device__ __forceinline__ T edge_row(const T* vec, const int32_t* enb, const T* ecf, long long n) {
+    const int4* pi = reinterpret_cast<const int4*>(enb + 12 * n);
+    const int4 i0 = __ldg(pi), i1 = __ldg(pi + 1), i2 = __ldg(pi + 2);
+    const int32_t q[12] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w, i2.x, i2.y, i2.z, i2.w};
+    T g[6];
+    load_coef(ecf, n, g);
+    T va[6], vb[6];
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        va[p] = (g[p] != T(0)) ? vec[q[2 * p]] : T(0);
+        vb[p] = (g[p] != T(0)) ? vec[q[2 * p + 1]] : T(0);
+    }
+    T acc = T(0);
+#pragma unroll
+    for (int p = 0; p < 6; ++p) acc += g[p] * (va[p] - vb[p]);
     return acc;
 }
 
@@ -652,6 +675,66 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         // shared memory.  The +-z neighbours (outside the tile in row order) get their
         // RK4 in the same pass as the voxel's own, as independent chains; any other
         // neighbour outside the tile is recomputed in the rare slow path.
+        // Anisotropic instances reach twelve more (edge) neighbours, eight of them
+        // across z: their u* goes through global memory instead (basis column 1,
+        // unused until the first Arnoldi step) with one more team barrier.
+        if (I.ecf) {
+            T* Us = Vb + ldV;
+            for (int tile = rank; tile < I.n_tiles; tile += P) {
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    const long long n = voxel(tile, v);
+                    if (n < N) {
+                        const T un = I.u[n], hn = hin[n];
+                        const uint8_t f = __ldg(I.vflags + n);
+                        sample_voxel(n, un, hn, step - 1);
+                        T p[5];
+                        params_of(n, p);
+                        const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
+                        T us, hs;
+                        rk4(I.model, un, hn, J, p, I.dt, us, hs);
+                        hout[n] = hs;
+                        Us[n] = us;
+                    }
+                }
+            }
+            if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+            for (int tile = rank; tile < I.n_tiles; tile += P) {
+                double ab = 0.0, ar = 0.0;
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    const long long n = voxel(tile, v);
+                    if (n < N) {
+                        const T us = __ldcg(Us + n);
+                        const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
+                        int32_t q[6];
+                        T c[6];
+                        load_nb(I.nb, n, q);
+                        row_coef(I.coef, I.cw, I.m6, n, c);
+                        T lap = T(0), dp = T(0), lapd = T(0);
+                        if (!rz) lap = lap_row(Us, us, q, c) + edge_row(Us, I.enb, I.ecf, n);
+                        if (I.dx) {
+                            dp = I.dx[n];
+                            if (!rz) lapd = lap_row(I.dx, dp, q, c) + edge_row(I.dx, I.enb, I.ecf, n);
+                        }
+                        const T x0 = us + dp;
+                        const T bn = us + I.half_dt * lap;
+                        const T ax = x0 - I.half_dt * (lap + lapd);
+                        const T rn = bn - ax;
+                        I.x[n] = x0;
+                        I.b[n] = bn;
+                        Vb[n] = rn;
+                        ab += (double)bn * (double)bn;
+                        ar += (double)rn * (double)rn;
+                    }
+                }
+                ab = warp_sum(ab);
+                ar = warp_sum(ar);
+                put(tile, 0, ab);
+                put(tile, 1, ar);
+                tile_done(tile, 2);
+            }
+        } else
         for (int tile = rank; tile < I.n_tiles; tile += P) {
             const long long base = (long long)tile * TILE;
             T us_reg[VPT], z4[VPT], z5[VPT];
@@ -795,7 +878,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                                 T c[6];
                                 load_nb(I.nb, n, q);
                                 row_coef(I.coef, I.cw, I.m6, n, c);
-                                const T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
+                                T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
+                                if (I.ecf && !rz) lap += edge_row(Vj, I.enb, I.ecf, n);
                                 const T w = sj * (vj - I.half_dt * lap);
                                 Vn[n] = w;
                                 wr[v] = w;
@@ -919,7 +1003,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             T c[6];
                             load_nb(I.nb, n, q);
                             row_coef(I.coef, I.cw, I.m6, n, c);
-                            const T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
+                            T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
+                            if (I.ecf && !rz) lap += edge_row(I.x, I.enb, I.ecf, n);
                             const T ax = xv - I.half_dt * lap;
                             const T r = I.b[n] - ax;
                             Vb[n] = r;
@@ -1049,6 +1134,8 @@ struct InstHost {
     void* coef = nullptr;
     void* cw = nullptr;
     void* m6 = nullptr;
+    void* enb = nullptr;
+    void* ecf = nullptr;
     void* vflags = nullptr;
     void* vparams = nullptr;
     void* stim = nullptr;
@@ -1077,7 +1164,7 @@ struct InstHost {
 };
 
 void free_inst(InstHost& h) {
-    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
+    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.enb, h.ecf, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
                     h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1166,6 +1253,13 @@ int validate_desc(const phs_instance_desc* d) {
     if (d->cw)
         for (long long i = 0; i < n; ++i)
             if (!std::isfinite(d->cw[i]) || (d->mask6[i] & 0xC0u)) return PHS_ERR_BAD_TABLE;
+    if ((d->nb_edge == nullptr) != (d->coef_edge == nullptr)) return PHS_ERR_BAD_ARG;
+    if (d->nb_edge) {
+        for (long long i = 0; i < 12 * n; ++i)
+            if (d->nb_edge[i] < 0 || d->nb_edge[i] >= n) return PHS_ERR_BAD_TABLE;
+        for (long long i = 0; i < 6 * n; ++i)
+            if (!std::isfinite(d->coef_edge[i])) return PHS_ERR_BAD_TABLE;
+    }
     return PHS_OK;
 }
 
@@ -1196,6 +1290,12 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
         if (cudaMemcpy(h.m6, d->mask6, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
     } else {
         if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6)) != PHS_OK) return fail(rc);
+    }
+    if (d->nb_edge) {
+        PHS_ALLOC(h.enb, n * 12 * sizeof(int32_t));
+        if (cudaMemcpy(h.enb, d->nb_edge, n * 12 * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(PHS_ERR_CUDA);
+        if ((rc = upload_converted<T>(&h.ecf, d->coef_edge, (long long)n * 6)) != PHS_OK) return fail(rc);
     }
     PHS_ALLOC(h.vflags, n);
     if (cudaMemcpy(h.vflags, d->vflags, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
@@ -1272,6 +1372,8 @@ InstDev<T> make_dev(const InstHost& h) {
     I.coef = (const T*)h.coef;
     I.cw = (const T*)h.cw;
     I.m6 = (const uint8_t*)h.m6;
+    I.enb = (const int32_t*)h.enb;
+    I.ecf = (const T*)h.ecf;
     I.vflags = (const uint8_t*)h.vflags;
     I.vparams = (const T*)h.vparams;
     I.stim = (const uint8_t*)h.stim;

@@ -14,6 +14,13 @@ same operator is kept matrix-free as a compacted table:
 
 so ``(L u)[n] = sum_k coef6[n,k] * (u[nb6[n,k]] - u[n])`` is the reference's
 row n (its diagonal is minus the sum of the neighbour entries).
+
+Anisotropic tensors (D0 != I) add the cross terms of simulation_gpu.py:171-217.
+The face ones (P_2d[:,6..8]) enter the +d neighbour with + and the -d neighbour
+with -, so they fold into ``coef6``; the edge ones (P_2d[:,9..14]) are six
+antisymmetric pairs per row, ``coef_edge[n,p] * (u[a] - u[b])`` with
+``(a, b) = nb_edge[n, 2p:2p+2]``.  Both forms keep the row sum at zero, as the
+reference's diagonal does.
 """
 import numpy as np
 
@@ -58,6 +65,11 @@ def locality_order(geometry_data, n, kind="rows"):
     return np.argsort(code, kind='stable')
 
 
+# Edge cross-term pairs (+ neighbour column, - neighbour column, P_2d column),
+# in the order of simulation/simulation_gpu.py:199-206.
+EDGE_PAIRS = ((6, 8, 9), (9, 7, 10), (14, 16, 11), (17, 15, 12), (10, 12, 13), (13, 11, 14))
+
+
 class CompiledInstance:
     """Host arrays + scalars of one instance, and the ctypes descriptor over them."""
 
@@ -95,6 +107,9 @@ class CompiledInstance:
         d.atol = self.atol
         d.maxiter = self.maxiter
         d.guess = int(getattr(self, "guess", 0))
+        edge = getattr(self, "coef_edge", None) is not None
+        d.nb_edge = _lib.ptr(self.nb_edge, _lib.ctypes.c_int32) if edge else None
+        d.coef_edge = _lib.ptr(self.coef_edge, _lib.ctypes.c_double) if edge else None
         self._desc = d
         return d
 
@@ -160,10 +175,10 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         raise ValueError("neighbor_id_2d must be (n_voxel, 18)")
     if np.any(nb[:, :6] < -1) or np.any(nb[:, :6] >= n):
         raise ValueError("neighbor_id_2d holds indices outside [-1, n_voxel)")
-    if np.any(P[:, 6:15] != 0):
-        raise NotImplementedError("anisotropic cross terms (P_2d columns 6..14 non-zero) are not "
-                                  "supported by this build; the reference's load_fiber always gives "
-                                  "D0 = I, for which they are zero")
+    cross_face = np.any(P[:, 6:9] != 0)
+    cross_edge = np.any(P[:, 9:15] != 0)
+    if cross_edge and (nb.shape[1] < 18 or np.any(nb[:, 6:18] < -1) or np.any(nb[:, 6:18] >= n)):
+        raise ValueError("edge cross terms need neighbor_id_2d columns 6..17 in [-1, n_voxel)")
     Delta = float(geometry_data['Delta'])
     model = int(simulation_parameters['heart_model_flag'])
     if model not in (0, 1):
@@ -184,7 +199,17 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
     c[node_flag == 4] = 0.0                       # permanent block
     nb6 = nb[:, :6].astype(np.int64).copy()
     nb6[nb6 == -1] = 0                            # the reference's -1 -> 0 remap
-    coef6 = (c / (4 * Delta ** 2))[:, None] * P[:, :6]
+    Dc = c / (4 * Delta ** 2)
+    coef6 = Dc[:, None] * P[:, :6]
+    if cross_face:
+        sign = np.array([1.0, -1.0, 1.0, -1.0, 1.0, -1.0])
+        coef6 = coef6 + (Dc[:, None] * P[:, [6, 6, 7, 7, 8, 8]]) * sign
+    nb_edge = coef_edge = None
+    if cross_edge:
+        pairs = np.array(EDGE_PAIRS)
+        nb_edge = nb[:, pairs[:, :2].ravel()].astype(np.int64)
+        nb_edge[nb_edge == -1] = 0
+        coef_edge = Dc[:, None] * P[:, pairs[:, 2]]
     vflags = np.zeros(n, dtype=np.uint8)
     s1 = np.atleast_1d(np.asarray(s1, dtype=np.int64)) if np.size(s1) else np.zeros(0, np.int64)
     s2 = np.atleast_1d(np.asarray(s2, dtype=np.int64)) if np.size(s2) else np.zeros(0, np.int64)
@@ -217,6 +242,9 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
             cw, mask6 = cw[order], mask6[order]
         if vparams is not None:
             vparams = np.ascontiguousarray(vparams[order])
+        if nb_edge is not None:
+            nb_edge = inv[nb_edge[order]]
+            coef_edge = coef_edge[order]
     u0, h0 = (0.0, 1.0) if model == 0 else (0.0, 0.0)
     return CompiledInstance(
         n_voxel=n, model=model, restart=int(min(restart, 50)), nb6=np.ascontiguousarray(nb6, dtype=np.int32),
@@ -226,4 +254,6 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol), atol=float(atol),
         maxiter=int(maxiter), time_scale=ts, Delta=Delta, order=order, inv=inv,
         guess=int((not full_cycles) if guess is None else bool(guess)),
-        cw=None if cw is None else np.ascontiguousarray(cw), mask6=None if mask6 is None else np.ascontiguousarray(mask6))
+        cw=None if cw is None else np.ascontiguousarray(cw), mask6=None if mask6 is None else np.ascontiguousarray(mask6),
+        nb_edge=None if nb_edge is None else np.ascontiguousarray(nb_edge, dtype=np.int32),
+        coef_edge=None if coef_edge is None else np.ascontiguousarray(coef_edge))

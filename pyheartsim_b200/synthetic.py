@@ -114,12 +114,34 @@ def model_parameters(model, n, c_voxel):
             'mu2_voxel': np.full(n, p['mu2']), 'c_voxel': np.asarray(c_voxel, dtype=np.float64)}
 
 
+def fibre_tensors(ijk, r=0.3, helix_deg=60.0):
+    """Rule-based fibre field of a shell centred on the origin, as diffusion
+    tensors D0 = r I + (1 - r) e e^T (the fiber_flag == 1 form of
+    simulation/equation_parts.py:28-29).  The fibre e lies in the wall's tangent
+    plane and turns with depth from +helix_deg (inner surface) to -helix_deg
+    (outer), measured from the circumferential direction.  Returns (n, 3, 3)."""
+    x = np.asarray(ijk, dtype=np.float64)
+    rho = np.linalg.norm(x, axis=1)
+    rad = x / np.maximum(rho, 1e-9)[:, None]
+    circ = np.cross(np.array([0.0, 0.0, 1.0]), rad)
+    small = np.linalg.norm(circ, axis=1) < 1e-6
+    circ[small] = np.array([1.0, 0.0, 0.0])
+    circ /= np.linalg.norm(circ, axis=1)[:, None]
+    lng = np.cross(rad, circ)
+    # depth through the wall from the radius, 0 inside .. 1 outside
+    t = (rho - rho.min()) / max(rho.max() - rho.min(), 1e-9)
+    a = np.deg2rad(helix_deg) * (1.0 - 2.0 * t)
+    e = np.cos(a)[:, None] * circ + np.sin(a)[:, None] * lng
+    return r * np.eye(3)[None] + (1.0 - r) * e[:, :, None] * e[:, None, :]
+
+
 def make_case(ijk, Delta, model, dt_phys, t_phys, s1_ids, *, c_phys=None, s2_ids=None, flag=4,
-              s1_t=0.0, s1_s2=0.0, start=10.0, cycle=300.0, node_flag=None, c_scale=None):
+              s1_t=0.0, s1_s2=0.0, start=10.0, cycle=300.0, node_flag=None, c_scale=None, D0=None):
     """The reference's (n_voxel, P_2d, geometry_data, simulation_parameters,
     arrhythmia_parameters) for one simulation, with the reference's time scaling
     for Aliev-Panfilov (configuration.py:145-157: dt, t_final and pacing times
-    divided by 6, c multiplied by 6)."""
+    divided by 6, c multiplied by 6).  ``D0``: (n, 3, 3) diffusion tensors
+    (default identity, the reference's load_fiber)."""
     n = ijk.shape[0]
     ts = 1 if model == 0 else 6
     nb = lattice_neighbors(ijk)
@@ -136,7 +158,7 @@ def make_case(ijk, Delta, model, dt_phys, t_phys, s1_ids, *, c_phys=None, s2_ids
           's1_t': s1_t / ts, 's1_s2_delta_t': s1_s2 / ts,
           'node_flag': np.zeros(n, dtype=np.int64) if node_flag is None else node_flag}
     par = model_parameters(model, n, c)
-    P = heart_model_equation_parts(sp, n, None, nb, par)
+    P = heart_model_equation_parts(sp, n, D0, nb, par)
     geom = {'neighbor_id_2d': nb, 'Delta': Delta, 'voxel': ijk * Delta}
     return n, P, geom, sp, ap
 

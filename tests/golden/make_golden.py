@@ -115,9 +115,18 @@ MS = dict(tau_in=0.3, tau_out=6.0, tau_open=120.0, tau_close=150.0, v_gate=0.13)
 AP = dict(k=8.0, a=0.15, epsilon_0=0.002, mu1=0.2, mu2=0.3)
 
 
+def fibre_D0(ijk, r=0.3):
+    """Anisotropic tensors D0 = r I + (1-r) e e^T with a smoothly rotating fibre
+    direction e (the fiber_flag == 1 form of simulation/equation_parts.py:28-29)."""
+    th = 0.35 * ijk[:, 0] + 0.2 * ijk[:, 2]
+    ph = 0.25 * ijk[:, 1]
+    e = np.stack([np.cos(th) * np.cos(ph), np.sin(th) * np.cos(ph), np.sin(ph)], axis=1)
+    return [r * np.eye(3) + (1 - r) * np.outer(v, v) for v in e]
+
+
 def build_case(simulation, vox, name, shape, model, dt_phys, t_phys, flag, s1_pred,
                s2_pred=None, s1_t=0.0, s1_s2=0.0, start=10.0, cycle=300.0,
-               node_flag_fn=None, c_base=None, Delta=0.4):
+               node_flag_fn=None, c_base=None, Delta=0.4, fibres=False):
     ijk = lattice(shape)
     n = ijk.shape[0]
     nb = vox.find_neighbor_voxel_ids(ijk)
@@ -141,7 +150,7 @@ def build_case(simulation, vox, name, shape, model, dt_phys, t_phys, flag, s1_pr
                "epsilon_0_voxel": np.full(n, AP["epsilon_0"]), "mu1_voxel": np.full(n, AP["mu1"]),
                "mu2_voxel": np.full(n, AP["mu2"]),
                "c_voxel": np.full(n, (1.6 if c_base is None else c_base) * ts)}
-    D0 = simulation.equation_parts.load_fiber(n)
+    D0 = fibre_D0(ijk) if fibres else simulation.equation_parts.load_fiber(n)
     P = simulation.equation_parts.heart_model_equation_parts(sp, n, D0, nb, par)
     return dict(name=name, ijk=ijk, voxel=voxel, nb=nb, Delta=Delta, sp=sp, ap=ap, par=par, P=P, D0=D0)
 
@@ -191,12 +200,19 @@ def main():
              s2_pred=lambda x: (x[:, 0] > 5) & (x[:, 1] > 5)),
         dict(name="sheet_ms_flag5", shape=(8, 8), model=0, dt_phys=0.5, t_phys=305.0, flag=5,
              s1_pred=lambda x: x[:, 0] == 0, s2_pred=lambda x: x[:, 0] == 7),
+        dict(name="slab_ms_fibres", shape=(7, 6, 4), model=0, dt_phys=0.1, t_phys=12.0, flag=4,
+             s1_pred=lambda x: (x[:, 0] < 2) & (x[:, 1] < 2), fibres=True,
+             node_flag_fn=lambda x: np.where((x[:, 0] == 4) & (x[:, 1] == 3), 4, 0)),
     ]
+    only = set(sys.argv[1:])
+    if only:
+        cases = [c for c in cases if c["name"] in only]
     out = {}
     for spec in cases:
         case = build_case(simulation, vox, **spec)
         name = case["name"]
         rec = {"ijk": case["ijk"], "voxel": case["voxel"], "neighbor_id_2d": case["nb"],
+               "D0": np.asarray(case["D0"], dtype=np.float64),
                "Delta": case["Delta"], "P_2d": case["P"],
                "s1": case["ap"]["s1_pacing_voxel_id"],
                "s2": np.asarray(case["ap"]["s2_pacing_voxel_id"], dtype=np.int64),
@@ -215,10 +231,14 @@ def main():
     for name, el in (("sheet_ms_flag4", np.array([[1.0, 1.0, 1.0], [4.0, 2.0, 1.0], [2.6, 4.4, 1.0],
                                                    [5.2, 5.2, 1.0], [0.4, 4.8, 2.0], [3.0, 0.2, 0.5]])),
                      ("slab_ap_flag1", np.array([[-1.0, 1.2, 0.6], [1.2, 3.6, 2.0], [2.4, -0.8, 0.4],
-                                                  [3.4, 1.2, 1.6], [1.0, 1.0, 0.6]]))):
+                                                  [3.4, 1.2, 1.6], [1.0, 1.0, 0.6]])),
+                     ("slab_ms_fibres", np.array([[-0.8, 0.9, 0.6], [1.4, 2.4, 2.1], [2.6, -0.9, 0.5],
+                                                   [1.2, 1.0, -1.1]]))):
+        if name not in out:
+            continue
         rec = out[name]
         case = dict(voxel=rec["voxel"], nb=rec["neighbor_id_2d"], Delta=rec["Delta"],
-                    D0=simulation.equation_parts.load_fiber(rec["voxel"].shape[0]),
+                    D0=[d for d in rec["D0"]],
                     par={"c_voxel": rec["P_2d"][:, 20]})
         with contextlib.redirect_stdout(io.StringIO()):
             e32 = run_egm(cp, simulation, case, rec["u_f32"], el, fp64=False)

@@ -33,7 +33,7 @@ def test_bindings_cover_header():
 
 def test_struct_layouts_match_c():
     # sizes fixed by include/phs.h (natural alignment, 64-bit)
-    assert ctypes.sizeof(_lib.InstanceDesc) == 200
+    assert ctypes.sizeof(_lib.InstanceDesc) == 216
     assert ctypes.sizeof(_lib.InstanceInfo) == 64
 
 

@@ -23,7 +23,7 @@ def test_plain_fp64_matches_reference_golden(name, cuda_device):
     np.testing.assert_array_equal(t, g["t_f64"])
 
 
-@pytest.mark.parametrize("case", ["sheet_ms", "slab_ap", "small_shell_ms"])
+@pytest.mark.parametrize("case", ["sheet_ms", "slab_ap", "small_shell_ms", "small_shell_ms_fibres"])
 def test_plain_fp64_matches_oracle(case, cuda_device):
     (n, P, geom, sp, ap), pdur = getattr(gpu_cases, case)()
     u, h, t, lat = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur, return_lat=True)
@@ -36,7 +36,7 @@ def test_plain_fp64_matches_oracle(case, cuda_device):
     np.testing.assert_array_equal(lat, lato)
 
 
-@pytest.mark.parametrize("case", ["sheet_ms", "slab_ap", "small_shell_ms"])
+@pytest.mark.parametrize("case", ["sheet_ms", "slab_ap", "small_shell_ms", "small_shell_ms_fibres"])
 def test_fast_fp32_lat_within_one_step(case, cuda_device):
     """FP32 state, FP64 dots, Givens early exit: LAT error <= 1 dt against FP64."""
     (n, P, geom, sp, ap), pdur = getattr(gpu_cases, case)()

@@ -55,8 +55,7 @@ def test_matrix_free_operator_equals_reference_csr(name):
     rng = np.random.default_rng(0)
     for _ in range(3):
         u = rng.standard_normal(c["n"])
-        mf = (inst.coef6 * (u[inst.nb6] - u[:, None])).sum(axis=1)
-        np.testing.assert_allclose(mf, L @ u, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(_table_laplacian(inst, u), L @ u, rtol=1e-12, atol=1e-12)
     # temporary block rows
     tb = (inst.vflags & 4) != 0
     np.testing.assert_array_equal(tb, nf == 3)
@@ -93,8 +92,45 @@ def test_compile_rejects_bad_tables():
         instance.compile_instance(c["n"], c["P_2d"], geom, c["sp"], c["ap"])
     P = c["P_2d"].copy()
     P[0, 9] = 0.5
-    with pytest.raises(NotImplementedError):
-        instance.compile_instance(c["n"], P, c["geom"], c["sp"], c["ap"])
+    geom = dict(c["geom"])
+    nb = geom["neighbor_id_2d"].copy()
+    nb[2, 7] = c["n"]
+    geom["neighbor_id_2d"] = nb
+    with pytest.raises(ValueError):                      # edge neighbours are checked when used
+        instance.compile_instance(c["n"], P, geom, c["sp"], c["ap"])
+
+
+def _table_laplacian(inst, u_caller):
+    """The operator the device applies, from the compiled tables (caller order)."""
+    u = u_caller if inst.order is None else u_caller[inst.order]
+    lap = (inst.coef6 * (u[inst.nb6] - u[:, None])).sum(axis=1)
+    if inst.coef_edge is not None:
+        e = inst.nb_edge
+        lap = lap + (inst.coef_edge * (u[e[:, 0::2]] - u[e[:, 1::2]])).sum(axis=1)
+    return inst.to_caller(lap)
+
+
+@pytest.mark.parametrize("reorder", [False, "rows", "morton"])
+def test_anisotropic_tables_reproduce_reference_laplacian(reorder):
+    """Fibre case (D0 != I, every cross term present): face cross terms folded
+    into coef6 plus six edge pairs give the reference's CSR L
+    (simulation_gpu.py:138-225, restated by the oracle) row for row."""
+    c = golden_cases.load("slab_ms_fibres")
+    P = c["P_2d"]
+    assert np.abs(P[:, 6:9]).max() > 0.1 and np.abs(P[:, 9:15]).max() > 0.1
+    inst = instance.compile_instance(c["n"], P, c["geom"], c["sp"], c["ap"], reorder=reorder)
+    assert inst.coef_edge is not None and inst.cw is None
+    Pc = P.copy()
+    Pc[c["ap"]["node_flag"] == 4, 20] = 0.0                 # permanent block, simulation_gpu.py:312-313
+    L = simulation_fp64.laplacian(Pc, c["geom"]["neighbor_id_2d"], c["geom"]["Delta"])
+    rng = np.random.default_rng(3)
+    for _ in range(3):
+        u = rng.standard_normal(c["n"])
+        np.testing.assert_allclose(_table_laplacian(inst, u), L @ u, rtol=0, atol=1e-12)
+    # isotropic case: no edge tables, same operator
+    c0 = golden_cases.load("slab_ap_flag1")
+    i0 = instance.compile_instance(c0["n"], c0["P_2d"], c0["geom"], c0["sp"], c0["ap"], reorder=reorder)
+    assert i0.coef_edge is None and i0.nb_edge is None
 
 
 @pytest.mark.parametrize("name", golden_cases.names())
@@ -111,7 +147,8 @@ def test_lattice_neighbors_and_P2d_match_reference(name):
             ("k_voxel", "a_voxel", "epsilon_0_voxel", "mu1_voxel", "mu2_voxel"))
     for col, k in zip(range(15, 20), keys):
         par[k] = g["P_2d"][:, col]
-    P = geometry.heart_model_equation_parts(c["sp"], n, geometry.load_fiber(n), nb, par)
+    D0 = list(g["D0"]) if "D0" in g.files else geometry.load_fiber(n)
+    P = geometry.heart_model_equation_parts(c["sp"], n, D0, nb, par)
     np.testing.assert_array_equal(P, g["P_2d"])
 
 

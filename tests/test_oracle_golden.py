@@ -25,7 +25,8 @@ def test_oracle_matches_reference_fp64_run(name):
 def test_egm_oracle_matches_reference(name):
     c = golden_cases.load(name)
     g = c["g"]
-    args = (g["egm_electrode_xyz"], g["voxel"], None, g["P_2d"][:, 20], g["u_f64"], float(g["Delta"]),
+    D0 = g["D0"] if "D0" in g.files else None      # None: the reference's D0 = I
+    args = (g["egm_electrode_xyz"], g["voxel"], D0, g["P_2d"][:, 20], g["u_f64"], float(g["Delta"]),
             g["neighbor_id_2d"])
     e_direct = egm_fp64.direct(*args)
     e_lead = egm_fp64.compute(*args)
