@@ -368,7 +368,9 @@ template <typename T>
 constexpr bool kWarpParts = sizeof(T) == 4;
 
 // ------------------------------------------------------------------ the kernel
-template <typename T, int VPT, int MINB>
+// EDGE: the launch carries anisotropic instances (edge cross terms); the
+// isotropic launches compile without that code.
+template <typename T, int VPT, int MINB, bool EDGE>
 __global__ void __launch_bounds__(kThreads, MINB)
 step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_map,
             long long n_steps_launch, unsigned int* abort_word) {
@@ -678,7 +680,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         // Anisotropic instances reach twelve more (edge) neighbours, eight of them
         // across z: their u* goes through global memory instead (basis column 1,
         // unused until the first Arnoldi step) with one more team barrier.
-        if (I.ecf) {
+        if (EDGE && I.ecf) {
             T* Us = Vb + ldV;
             for (int tile = rank; tile < I.n_tiles; tile += P) {
 #pragma unroll
@@ -879,7 +881,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                                 load_nb(I.nb, n, q);
                                 row_coef(I.coef, I.cw, I.m6, n, c);
                                 T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
-                                if (I.ecf && !rz) lap += edge_row(Vj, I.enb, I.ecf, n);
+                                if (EDGE && I.ecf && !rz) lap += edge_row(Vj, I.enb, I.ecf, n);
                                 const T w = sj * (vj - I.half_dt * lap);
                                 Vn[n] = w;
                                 wr[v] = w;
@@ -1004,7 +1006,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             load_nb(I.nb, n, q);
                             row_coef(I.coef, I.cw, I.m6, n, c);
                             T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
-                            if (I.ecf && !rz) lap += edge_row(I.x, I.enb, I.ecf, n);
+                            if (EDGE && I.ecf && !rz) lap += edge_row(I.x, I.enb, I.ecf, n);
                             const T ax = xv - I.half_dt * lap;
                             const T r = I.b[n] - ax;
                             Vb[n] = r;
@@ -1107,20 +1109,24 @@ constexpr int kVptF64 = 1;
 
 // Compiled step-kernel variants: same algorithm and tiling, different register
 // budgets (__launch_bounds__ minimum CTAs per SM).  The autotuner picks one.
+// Each exists without and with the anisotropic edge terms.
 using StepFnF = void (*)(const InstDev<float>*, const int4*, long long, unsigned int*);
 using StepFnD = void (*)(const InstDev<double>*, const int4*, long long, unsigned int*);
-const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2>, step_kernel<float, kVptF32, 3>,
-                            step_kernel<float, kVptF32, 4>};
+const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2, false>, step_kernel<float, kVptF32, 3, false>,
+                            step_kernel<float, kVptF32, 4, false>};
+const StepFnF kStepF32Edge[] = {step_kernel<float, kVptF32, 2, true>, step_kernel<float, kVptF32, 3, true>,
+                                step_kernel<float, kVptF32, 4, true>};
 const int kMinbF32[] = {2, 3, 4};
-const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2>, step_kernel<double, kVptF64, 3>};
+const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2, false>, step_kernel<double, kVptF64, 3, false>};
+const StepFnD kStepF64Edge[] = {step_kernel<double, kVptF64, 2, true>, step_kernel<double, kVptF64, 3, true>};
 const int kMinbF64[] = {2, 3};
 constexpr int kNumF32 = 3, kNumF64 = 2;
 constexpr int kDefaultF32 = 1, kDefaultF64 = 0;
 
 template <typename T>
-const void* step_fn(int variant) {
-    if (sizeof(T) == 8) return (const void*)kStepF64[variant];
-    return (const void*)kStepF32[variant];
+const void* step_fn(int variant, bool edge = false) {
+    if (sizeof(T) == 8) return edge ? (const void*)kStepF64Edge[variant] : (const void*)kStepF64[variant];
+    return edge ? (const void*)kStepF32Edge[variant] : (const void*)kStepF32[variant];
 }
 
 struct InstHost {
@@ -1190,6 +1196,7 @@ struct phs_engine {
     std::vector<int> act;
     std::vector<std::pair<size_t, int>> waves;
     int plan_cps = -1;
+    bool plan_edge = false;  // the plan launches the edge-term kernel
     // CUDA graphs of the launch sequence, keyed by steps per launch
     std::map<long long, cudaGraphExec_t> graphs;
     bool graphs_ok = true;
@@ -1202,8 +1209,8 @@ struct phs_engine {
 namespace {
 
 template <typename T>
-int occupancy_for(int* ctas, int variant) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_fn<T>(variant), kThreads, 0);
+int occupancy_for(int* ctas, int variant, bool edge = false) {
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_fn<T>(variant, edge), kThreads, 0);
     if (e != cudaSuccess) { set_last_error("occupancy", e); return PHS_ERR_CUDA; }
     return PHS_OK;
 }
@@ -1487,7 +1494,7 @@ cudaError_t launch_waves(phs_engine* e, long long n_steps, cudaStream_t stream) 
         long long ns = n_steps;
         unsigned int* ab = e->abort_word;
         void* args[] = {(void*)&dd, (void*)&mp, (void*)&ns, (void*)&ab};
-        cudaError_t ce = cudaLaunchKernelExC(&cfg, step_fn<T>(variant_of<T>(e)), args);
+        cudaError_t ce = cudaLaunchKernelExC(&cfg, step_fn<T>(variant_of<T>(e), e->plan_edge), args);
         if (ce != cudaSuccess) return ce;
     }
     return cudaSuccess;
@@ -1495,7 +1502,7 @@ cudaError_t launch_waves(phs_engine* e, long long n_steps, cudaStream_t stream) 
 
 // (Re)build the launch plan: device descriptors, team map and waves.
 template <typename T>
-int build_plan(phs_engine* e, int cps) {
+int build_plan(phs_engine* e, int cps, bool edge) {
     // earlier launches may still read the old descriptors
     PHS_CUDA_TRY(cudaDeviceSynchronize());
     const int G = e->sms * cps;
@@ -1506,6 +1513,7 @@ int build_plan(phs_engine* e, int cps) {
     e->waves.clear();
     drop_graphs(e);
     e->plan_cps = cps;
+    e->plan_edge = edge;
     e->dirty = false;
     if (act.empty()) return PHS_OK;
     std::vector<InstDev<T>> descs;
@@ -1560,14 +1568,18 @@ template <typename T>
 int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t stream, bool sync) {
     if (e->broken) return PHS_ERR_STATE;
     if (n_steps <= 0) return PHS_OK;
+    // the edge-term kernel only when an unfinished instance is anisotropic
+    bool edge = false;
+    for (const auto& h : e->inst)
+        if (h.used && !h.finished && h.enb) edge = true;
     int occ = 0;
-    int rc = occupancy_for<T>(&occ, variant_of<T>(e));
+    int rc = occupancy_for<T>(&occ, variant_of<T>(e), edge);
     if (rc != PHS_OK) return rc;
     if (occ < 1) return PHS_ERR_CUDA;
     if (ctas_per_sm <= 0) ctas_per_sm = e->default_cps;
     int cps = (ctas_per_sm > 0) ? std::min(ctas_per_sm, occ) : occ;
-    if (e->dirty || cps != e->plan_cps) {
-        rc = build_plan<T>(e, cps);
+    if (e->dirty || cps != e->plan_cps || edge != e->plan_edge) {
+        rc = build_plan<T>(e, cps, edge);
         if (rc != PHS_OK) return rc;
     }
     const std::vector<int>& act = e->act;

@@ -57,3 +57,30 @@ def test_repeat_is_bit_identical(cuda_device):
     b = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur, dtype=np.float32, fast=True)
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+def test_isotropic_instance_unchanged_beside_anisotropic(cuda_device):
+    """A batch holding an anisotropic instance launches the edge-term kernel; the
+    isotropic instance next to it gives the same history as when it runs alone
+    (the kernel without edge terms)."""
+    from pyheartsim_b200 import instance
+    from pyheartsim_b200.engine import BatchedEngine
+    (n, P, geom, sp, ap), pdur = gpu_cases.small_shell_ms(t_phys=15.0)
+    (nf, Pf, geomf, spf, apf), _ = gpu_cases.small_shell_ms(t_phys=15.0, fibres=True)
+    kw = dict(full_cycles=False, tol=1e-7, restart=20, pacing_duration=pdur)
+    iso = instance.compile_instance(n, P, geom, dict(sp), dict(ap), **kw)
+    ani = instance.compile_instance(nf, Pf, geomf, dict(spf), dict(apf), **kw)
+    assert iso.coef_edge is None and ani.coef_edge is not None
+    alone = BatchedEngine()
+    s0 = alone.add(iso)
+    while not alone.finished(s0):
+        alone.advance(50)
+    ref = alone.history(s0)
+    alone.close()
+    mix = BatchedEngine()
+    a, b = mix.add(iso), mix.add(ani)
+    while not (mix.finished(a) and mix.finished(b)):
+        mix.advance(50)
+    np.testing.assert_array_equal(mix.history(a), ref)
+    assert mix.info(b)["status"] == 0
+    mix.close()
