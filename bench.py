@@ -31,9 +31,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
 # DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) on a 16-shell, 2.37M-voxel launch at 4.0 Arnoldi steps per
-# solve (profiles/step_kernel_16shells_full.md); scaled to a full launch below.
-STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 363.5
+# dram__bytes_write.sum, median of 24 full-size launches of this batch at 2.40
+# Arnoldi steps per solve, profiles/step_kernel_64shells_dram_fullsize.md);
+# multiplied by the voxels and steps of one launch below.
+STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 219.5
+STEP_TRAFFIC_ARNOLDI_PER_SOLVE = 2.40
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
 
 
@@ -60,6 +62,8 @@ def parse():
     p.add_argument("--egm-ne", type=int, default=2048)
     p.add_argument("--egm-T", type=int, default=1000)
     p.add_argument("--egm-only", action="store_true", help="run only the electrogram leg (profiling case)")
+    p.add_argument("--aniso-only", action="store_true", help="run only the anisotropic (fibre) leg")
+    p.add_argument("--aniso-instances", type=int, default=16)
     return p.parse_args()
 
 
@@ -272,8 +276,9 @@ def run_b200(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
                          "traffic": STEP_TRAFFIC_BYTES_PER_VOXEL_STEP * float(ns.sum()) * S,
-                         "traffic_source": "ncu dram bytes per voxel-step (2.37M-voxel capture, k=4.0) x voxels x steps per launch",
-                         "kernel": "step_kernel<float,4>",
+                         "traffic_source": ("ncu dram__bytes_read+write per voxel-step of full-size launches of this "
+                                            f"batch (k={STEP_TRAFFIC_ARNOLDI_PER_SOLVE}) x voxels x steps per launch"),
+                         "kernel": step_kernel_name(tune),
                          "bytes_per_voxel_step": alg_bytes / local_vs},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "phases_ms_per_step": phases}
@@ -283,6 +288,7 @@ def run_b200(args):
         if rank == 0 and world == 1:
             line["plain_fp64"] = plain_leg(args, batch, value, dev)
             line["accuracy"] = accuracy_leg(dev, args.tol)
+            line["anisotropic"] = aniso_leg(args, dev, tune, count=args.aniso_instances)
             del batch, insts
             line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
             line["electrogram"] = egm_leg(args, dev)
@@ -293,6 +299,15 @@ def run_b200(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def step_kernel_name(tune):
+    """Template arguments of the step-kernel variant the timed launches used."""
+    from pyheartsim_b200.engine import step_variants
+    from pyheartsim_b200 import _lib
+    var = {v: minb for v, minb, _ in step_variants(_lib.PREC_F32)}
+    v = tune["best"][0] if tune is not None else None
+    return f"step_kernel<float,4,{var[v]},false>" if v in var else "step_kernel<float,4,default,false>"
 
 
 def phase_profile(eng, slots, S, stream):
@@ -335,7 +350,9 @@ def e2e_leg(args, insts, ns, steps, dev):
     t0 = time.perf_counter()
     eng = BatchedEngine(_lib.PREC_F32)
     slots = [eng.add(x) for x in insts]
-    h2d = sum(x.nb6.nbytes + x.coef6.nbytes + x.vflags.nbytes + x.stim.nbytes for x in insts)
+    h2d = sum(x.nb6.nbytes + (x.cw.nbytes + x.mask6.nbytes if x.cw is not None else x.coef6.nbytes)
+              + x.vflags.nbytes + x.stim.nbytes + (x.vparams.nbytes if x.vparams is not None else 0)
+              for x in insts)
     S = max(1, args.steps_per_launch)
     done = 0
     while done < steps:
@@ -384,6 +401,65 @@ def plain_leg(args, batch, fast_value, dev):
     return {"value": v, "unit": "voxel-steps/s", "instance": i, "voxels": int(meta["n"]), "steps": steps,
             "arnoldi_per_solve": info["arnoldi_steps"] / max(info["solves"], 1),
             "speedup_batched_fp32": fast_value / v}
+
+
+def aniso_leg(args, dev, tune=None, count=16):
+    """Anisotropic tensors (rule-based fibre field, every cross term present):
+    ``count`` seeded shells of n_min..n_max voxels through the edge-term kernel,
+    warmed up and timed like the main batch (CUDA events on the launch stream)."""
+    import torch
+    from pyheartsim_b200 import _lib, roofline, workloads
+    from pyheartsim_b200.engine import BatchedEngine
+    batch = workloads.batched_shells(count, args.n_min, args.n_max, args.seed + 11, tol=args.tol,
+                                     t_phys=args.t_phys, fibres=True)
+    insts = [b[0] for b in batch]
+    ns = np.array([m["n"] for _, m in batch], dtype=np.int64)
+    eng = BatchedEngine(_lib.PREC_F32)
+    if tune is not None:
+        eng.configure(variant=tune["best"][0], ctas_per_sm=tune["best"][1])
+    slots = [eng.add(x) for x in insts]
+    stream = torch.cuda.current_stream(dev)
+    S = max(1, args.steps_per_launch)
+    for _ in range(max(1, 300 // S)):
+        eng.advance(S, stream=stream, sync=False)
+    eng.set_profile(True)
+    for _ in range(2):
+        eng.rebalance()
+        eng.advance(S, stream=stream, sync=False)
+    eng.rebalance()
+    eng.set_profile(False)
+    eng.advance(S, stream=stream, sync=False)
+    torch.cuda.synchronize(dev)
+    info0 = [eng.info(s) for s in slots]
+    launches0 = eng.launches()
+    K = max(1, 100 // S) * S
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(K // S):
+        eng.advance(S, stream=stream, sync=False)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1)
+    launches = eng.launches() - launches0
+    info1 = [eng.info(s) for s in slots]
+    eng.close()
+    for a, b in zip(info0, info1):
+        assert b["step"] - a["step"] == K, "an instance finished inside the timed window"
+    k_sum = np.array([b["arnoldi_steps"] - a["arnoldi_steps"] for a, b in zip(info0, info1)], dtype=np.float64)
+    k_sq = np.array([b["arnoldi_sq"] - a["arnoldi_sq"] for a, b in zip(info0, info1)], dtype=np.float64)
+    solves = np.array([b["solves"] - a["solves"] for a, b in zip(info0, info1)], dtype=np.float64)
+    alg = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, x.cw is not None, bool(x.guess), edge=True)
+                    for n, ks, kq, sv, x in zip(ns, k_sum, k_sq, solves, insts)))
+    pk, pk_src = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
+    return {"value": float(ns.sum()) * K / (ms / 1e3), "unit": "voxel-steps/s", "instances": int(count),
+            "voxels": int(ns.sum()), "steps": int(K), "ms_per_step": ms / K, "gpu_launches": int(launches),
+            "arnoldi_per_solve": float(k_sum.sum() / max(solves.sum(), 1)),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+                         "bytes_per_voxel_step": alg / (float(ns.sum()) * K)},
+            "fibres": "D0 = 0.3 I + 0.7 e e^T, helix +-60 deg through the wall"}
 
 
 def accuracy_leg(dev, tol):
@@ -555,6 +631,12 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"electrogram": egm_leg(args, dev)}), flush=True)
+        return 0
+    if args.aniso_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"anisotropic": aniso_leg(args, dev, count=args.aniso_instances)}), flush=True)
         return 0
     return run_b200(args)
 

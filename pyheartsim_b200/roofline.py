@@ -18,6 +18,11 @@ A solve with k Arnoldi steps therefore costs
   B(k) = RHS + (k + 2) s + k (5 s + 24 + cb) + s k (k - 1),
 e.g. 81 + 68 k + 4 k^2 bytes in FP32 with six stored coefficients, and
 62 + 49 k + 4 k^2 with isotropic rows.
+
+Anisotropic rows (edge cross terms) add the edge table, 12 int32 indices and
+six coefficients = 48 + 6 s, to every operator application (the RHS and each
+A_j), and their RHS phase passes u* through memory (write + read, 2 s) and
+reads the flags twice (+1): in FP32 +97 bytes per step and +72 per Arnoldi step.
 """
 
 
@@ -29,7 +34,11 @@ def bytes_rhs(s, cb):
     return 6 * s + 25 + cb
 
 
-def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False):
+def edge_bytes(s):
+    return 48 + 6 * s
+
+
+def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False, edge=False):
     """Total algorithmic bytes of ``steps`` steps of an instance with ``voxels``
     voxels whose solves took ``k_sum`` Arnoldi steps in total (``k_sq_sum`` =
     sum of squares).  Steps that needed no iteration still run the RHS phase
@@ -39,6 +48,8 @@ def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, 
                  + s * k_sum)
     if guess:     # read the increment in the RHS phase; read and rewrite it in the final update
         per_voxel += steps * s + 2 * s * (solves or 0)
+    if edge:
+        per_voxel += steps * (edge_bytes(s) + 2 * s + 1) + edge_bytes(s) * k_sum
     return voxels * per_voxel
 
 

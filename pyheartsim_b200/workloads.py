@@ -31,8 +31,9 @@ def _shell_scaled(n_target, seed, Delta=0.4, wall=3):
 
 
 def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-5, restart=20,
-               save_h=False, pacing_ms=2.0):
-    """Reference-style inputs + the compiled instance of shell ``i``."""
+               save_h=False, pacing_ms=2.0, fibres=False):
+    """Reference-style inputs + the compiled instance of shell ``i`` (``fibres``:
+    rule-based fibre field, anisotropic D0)."""
     rng = np.random.default_rng(seed * 1000 + i)
     ijk = _shell_scaled(n_target, seed * 1000 + i)
     nb = lattice_neighbors(ijk)
@@ -43,12 +44,13 @@ def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-
     s1 = np.where(np.sum((ijk - centre) ** 2, axis=1) <= 9)[0]
     model = i % 2
     dt_phys = 0.05 if model == 0 else 0.02
-    n, P, geom, sp, ap = synthetic.make_case(ijk, 0.4, model, dt_phys, t_phys, s1, flag=4, c_scale=c_scale)
+    D0 = synthetic.fibre_tensors(ijk) if fibres else None
+    n, P, geom, sp, ap = synthetic.make_case(ijk, 0.4, model, dt_phys, t_phys, s1, flag=4, c_scale=c_scale, D0=D0)
     inst = _instance.compile_instance(n, P, geom, sp, ap, full_cycles=not fast, tol=tol, atol=1e-5,
                                       restart=restart if fast else 50, pacing_duration=pacing_ms / sp['time_scale'],
                                       save_h=save_h)
     return inst, (n, P, geom, sp, ap), {"index": i, "n": n, "model": model, "scar": cov,
-                                        "pacing_ms": pacing_ms}
+                                        "pacing_ms": pacing_ms, "fibres": bool(fibres)}
 
 
 def _build_one(args):
