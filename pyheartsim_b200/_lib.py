@@ -33,6 +33,7 @@ CFG_VARIANT = 1
 CFG_CTAS_PER_SM = 2
 CFG_PROFILE = 3
 CFG_TEST_TEAM_OVERCOUNT = 4
+CFG_AUTO_BALANCE = 5
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
                  "check", "check_wait", "copy", "step_wait", "steps", "arnoldi_iters", "team_ctas")
 

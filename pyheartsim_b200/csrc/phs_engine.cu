@@ -5,11 +5,10 @@
 // barrier, so instances of different sizes progress independently inside one
 // launch.  Per step and instance:
 //
-//   RHS phase   fused RK4 reaction (simulation/simulation_gpu.py:27-43, 71-130)
-//               evaluated in registers for the voxel and its six neighbours, fed
-//               straight into the Crank-Nicolson right-hand side
-//               b = u* + dt/2 L u*  (simulation/simulation_gpu.py:245) and the
-//               initial residual r0 = b - A u*  (A = I - dt/2 L, :321-322)
+//   RHS phase   RK4 reaction (simulation/simulation_gpu.py:27-43, 71-130) of
+//               every voxel, then, after a team barrier, the Crank-Nicolson
+//               right-hand side b = u* + dt/2 L u*  (simulation/simulation_gpu.py:245)
+//               and the initial residual r0 = b - A x0  (A = I - dt/2 L, :321-322)
 //   GMRES       restarted GMRES on A (CuPy semantics of the reference's call at
 //               simulation/simulation_gpu.py:253): classical Gram-Schmidt, the
 //               Hessenberg least-squares solved by Givens rotations on device,
@@ -382,7 +381,6 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     __shared__ InstDev<T> I;
     __shared__ SharedCtl ctl;
     __shared__ double shc[kMaxRestart + 1];
-    __shared__ T ustar_tile[TILE];
     __shared__ long long sh_step0;
     __shared__ int sh_id_save, sh_pending, sh_hbuf, sh_status;
 
@@ -673,164 +671,59 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         const T* hin = hbuf ? I.h1 : I.h0;
         T* hout = hbuf ? I.h0 : I.h1;
 
-        // ================= RHS phase: fused RK4 + b + r0.  The tile's own u* stay in
-        // shared memory.  The +-z neighbours (outside the tile in row order) get their
-        // RK4 in the same pass as the voxel's own, as independent chains; any other
-        // neighbour outside the tile is recomputed in the rare slow path.
-        // Anisotropic instances reach twelve more (edge) neighbours, eight of them
-        // across z: their u* goes through global memory instead (basis column 1,
-        // unused until the first Arnoldi step) with one more team barrier.
-        if (EDGE && I.ecf) {
-            T* Us = Vb + ldV;
-            for (int tile = rank; tile < I.n_tiles; tile += P) {
-#pragma unroll
-                for (int v = 0; v < VPT; ++v) {
-                    const long long n = voxel(tile, v);
-                    if (n < N) {
-                        const T un = I.u[n], hn = hin[n];
-                        const uint8_t f = __ldg(I.vflags + n);
-                        sample_voxel(n, un, hn, step - 1);
-                        T p[5];
-                        params_of(n, p);
-                        const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
-                        T us, hs;
-                        rk4(I.model, un, hn, J, p, I.dt, us, hs);
-                        hout[n] = hs;
-                        Us[n] = us;
-                    }
-                }
-            }
-            if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
-            for (int tile = rank; tile < I.n_tiles; tile += P) {
-                double ab = 0.0, ar = 0.0;
-#pragma unroll
-                for (int v = 0; v < VPT; ++v) {
-                    const long long n = voxel(tile, v);
-                    if (n < N) {
-                        const T us = __ldcg(Us + n);
-                        const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
-                        int32_t q[6];
-                        T c[6];
-                        load_nb(I.nb, n, q);
-                        row_coef(I.coef, I.cw, I.m6, n, c);
-                        T lap = T(0), dp = T(0), lapd = T(0);
-                        if (!rz) lap = lap_row(Us, us, q, c) + edge_row(Us, I.enb, I.ecf, n);
-                        if (I.dx) {
-                            dp = I.dx[n];
-                            if (!rz) lapd = lap_row(I.dx, dp, q, c) + edge_row(I.dx, I.enb, I.ecf, n);
-                        }
-                        const T x0 = us + dp;
-                        const T bn = us + I.half_dt * lap;
-                        const T ax = x0 - I.half_dt * (lap + lapd);
-                        const T rn = bn - ax;
-                        I.x[n] = x0;
-                        I.b[n] = bn;
-                        Vb[n] = rn;
-                        ab += (double)bn * (double)bn;
-                        ar += (double)rn * (double)rn;
-                    }
-                }
-                ab = warp_sum(ab);
-                ar = warp_sum(ar);
-                put(tile, 0, ab);
-                put(tile, 1, ar);
-                tile_done(tile, 2);
-            }
-        } else
+        // ================= RHS phase.  Pass 1: RK4 reaction of every voxel of the
+        // team; u* goes to basis column 1 (unused until the first Arnoldi step).
+        // Pass 2, after a team barrier: b = u* + dt/2 L u*, the initial guess and
+        // r0 = b - A x0 -> V0, gathering u* of the neighbours from memory.  (A
+        // fused form that kept a tile's u* in shared memory and recomputed the RK4
+        // of neighbours outside the tile did three RK4 per voxel in row order and
+        // was 17 % slower over the batch.)
+        T* Us = Vb + ldV;
         for (int tile = rank; tile < I.n_tiles; tile += P) {
-            const long long base = (long long)tile * TILE;
-            T us_reg[VPT], z4[VPT], z5[VPT];
-            unsigned zfar = 0u;
-#pragma unroll 2
+#pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
-                us_reg[v] = T(0);
-                z4[v] = T(0);
-                z5[v] = T(0);
                 if (n < N) {
                     const T un = I.u[n], hn = hin[n];
                     const uint8_t f = __ldg(I.vflags + n);
-                    const bool rz = tb && (f & PHS_VFLAG_TBLOCK);
-                    const int2 qz = __ldg(reinterpret_cast<const int2*>(I.nb + 6 * n + 4));
-                    bool f4 = false, f5 = false;
-                    if (!rz) {
-                        if (I.cw) {
-                            const unsigned mk = __ldg(I.m6 + n);
-                            f4 = (mk & 16u) != 0u;
-                            f5 = (mk & 32u) != 0u;
-                        } else {
-                            f4 = I.coef[6 * n + 4] != T(0);
-                            f5 = I.coef[6 * n + 5] != T(0);
-                        }
-                        f4 = f4 && ((long long)qz.x - base < 0 || (long long)qz.x - base >= TILE);
-                        f5 = f5 && ((long long)qz.y - base < 0 || (long long)qz.y - base >= TILE);
-                    }
-                    const long long q4 = f4 ? qz.x : n, q5 = f5 ? qz.y : n;
-                    const T u4 = I.u[q4], h4 = hin[q4], u5 = I.u[q5], h5 = hin[q5];
-                    const uint8_t fl4 = __ldg(I.vflags + q4), fl5 = __ldg(I.vflags + q5);
                     sample_voxel(n, un, hn, step - 1);
-                    T p[5], p4[5], p5[5];
+                    T p[5];
                     params_of(n, p);
-                    params_of(q4, p4);
-                    params_of(q5, p5);
                     const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
-                    const T J4 = (fl4 & stim_bits & 3u) ? I.jmag : T(0);
-                    const T J5 = (fl5 & stim_bits & 3u) ? I.jmag : T(0);
-                    T us, hs, us4, hs4, us5, hs5;
+                    T us, hs;
                     rk4(I.model, un, hn, J, p, I.dt, us, hs);
-                    rk4(I.model, u4, h4, J4, p4, I.dt, us4, hs4);
-                    rk4(I.model, u5, h5, J5, p5, I.dt, us5, hs5);
                     hout[n] = hs;
-                    us_reg[v] = us;
-                    z4[v] = us4;
-                    z5[v] = us5;
-                    zfar |= (f4 ? 1u : 0u) << (2 * v);
-                    zfar |= (f5 ? 2u : 0u) << (2 * v);
-                    ustar_tile[v * kThreads + threadIdx.x] = us;
+                    Us[n] = us;
                 }
             }
-            __syncthreads();
+        }
+        pending = -1;
+        if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+        for (int tile = rank; tile < I.n_tiles; tile += P) {
             double ab = 0.0, ar = 0.0;
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
                 if (n < N) {
-                    const T us = us_reg[v];
+                    const T us = __ldcg(Us + n);
                     const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
                     int32_t q[6];
                     T c[6];
                     load_nb(I.nb, n, q);
                     row_coef(I.coef, I.cw, I.m6, n, c);
-                    T lap = T(0);
+                    T lap = T(0), dp = T(0), lapd = T(0);
                     if (!rz) {
-#pragma unroll
-                        for (int k = 0; k < 6; ++k) {
-                            if (c[k] == T(0)) continue;
-                            const long long off = (long long)q[k] - base;
-                            T usq;
-                            if (off >= 0 && off < TILE) {
-                                usq = ustar_tile[off];
-                            } else if (k == 4 && (zfar >> (2 * v) & 1u)) {
-                                usq = z4[v];
-                            } else if (k == 5 && (zfar >> (2 * v) & 2u)) {
-                                usq = z5[v];
-                            } else {
-                                // slow path: a +-x / +-y neighbour outside the tile
-                                T pq[5];
-                                params_of(q[k], pq);
-                                const T Jq = (__ldg(I.vflags + q[k]) & stim_bits & 3u) ? I.jmag : T(0);
-                                T hsq;
-                                rk4(I.model, I.u[q[k]], hin[q[k]], Jq, pq, I.dt, usq, hsq);
-                            }
-                            lap += c[k] * (usq - us);
-                        }
+                        lap = lap_row(Us, us, q, c);
+                        if (EDGE && I.ecf) lap += edge_row(Us, I.enb, I.ecf, n);
                     }
                     // initial guess: u* (the reference's x0), or u* plus the previous
                     // step's diffusion increment when dx is kept
-                    T dp = T(0), lapd = T(0);
                     if (I.dx) {
                         dp = I.dx[n];
-                        if (!rz) lapd = lap_row(I.dx, dp, q, c);
+                        if (!rz) {
+                            lapd = lap_row(I.dx, dp, q, c);
+                            if (EDGE && I.ecf) lapd += edge_row(I.dx, I.enb, I.ecf, n);
+                        }
                     }
                     const T x0 = us + dp;
                     const T bn = us + I.half_dt * lap;
@@ -848,9 +741,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             put(tile, 0, ab);
             put(tile, 1, ar);
             tile_done(tile, 2);
-            __syncthreads();   // ustar_tile is rewritten by the next tile
         }
-        pending = -1;
         mark(PF_RHS);
         if (!team_sync(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
         int act = read_action();
@@ -1121,7 +1012,7 @@ const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2, false>, step_kernel<
 const StepFnD kStepF64Edge[] = {step_kernel<double, kVptF64, 2, true>, step_kernel<double, kVptF64, 3, true>};
 const int kMinbF64[] = {2, 3};
 constexpr int kNumF32 = 3, kNumF64 = 2;
-constexpr int kDefaultF32 = 1, kDefaultF64 = 0;
+constexpr int kDefaultF32 = 2, kDefaultF64 = 0;   // FP32: 64 registers, 4 CTAs/SM (the autotuner's pick on B200)
 
 template <typename T>
 const void* step_fn(int variant, bool edge = false) {
@@ -1197,6 +1088,9 @@ struct phs_engine {
     std::vector<std::pair<size_t, int>> waves;
     int plan_cps = -1;
     bool plan_edge = false;  // the plan launches the edge-term kernel
+    bool auto_balance = true;  // rebalance on the 2nd and 3rd advance after the instance set changes
+    int auto_left = 0;
+    long long auto_mark = 0;   // launch count when the set changed / at the last automatic rebalance
     // CUDA graphs of the launch sequence, keyed by steps per launch
     std::map<long long, cudaGraphExec_t> graphs;
     bool graphs_ok = true;
@@ -1368,6 +1262,8 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     }
     e->inst[s] = h;
     e->dirty = true;
+    e->auto_left = 2;
+    e->auto_mark = e->launches;
     *slot = s;
     return PHS_OK;
 }
@@ -1568,6 +1464,12 @@ template <typename T>
 int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t stream, bool sync) {
     if (e->broken) return PHS_ERR_STATE;
     if (n_steps <= 0) return PHS_OK;
+    if (e->auto_balance && e->auto_left > 0 && e->launches > e->auto_mark) {
+        const int rb = phs_engine_rebalance(e);
+        if (rb != PHS_OK) return rb;
+        e->auto_left -= 1;
+        e->auto_mark = e->launches;
+    }
     // the edge-term kernel only when an unfinished instance is anisotropic
     bool edge = false;
     for (const auto& h : e->inst)
@@ -1696,6 +1598,8 @@ int phs_instance_remove(phs_engine* e, int slot) {
     cudaDeviceSynchronize();
     free_inst(e->inst[slot]);
     e->dirty = true;
+    e->auto_left = 2;
+    e->auto_mark = e->launches;
     return PHS_OK;
 }
 
@@ -1829,6 +1733,9 @@ int phs_engine_config(phs_engine* e, int key, int64_t value) {
         case PHS_CFG_CTAS_PER_SM:
             if (value < 0 || value > 32) return PHS_ERR_BAD_ARG;
             e->default_cps = (int)value;
+            return PHS_OK;
+        case PHS_CFG_AUTO_BALANCE:
+            e->auto_balance = value != 0;
             return PHS_OK;
         case PHS_CFG_TEST_TEAM_OVERCOUNT:
             e->test_overcount = value != 0;

@@ -91,9 +91,13 @@ class BatchedEngine:
     def config(self, key, value):
         _lib.check(_lib.lib().phs_engine_config(self._h, int(key), int(value)), "phs_engine_config")
 
-    def configure(self, variant=None, ctas_per_sm=None):
-        """Select the step-kernel variant and the CTAs per SM used by advance()."""
+    def configure(self, variant=None, ctas_per_sm=None, auto_balance=None):
+        """Select the step-kernel variant and the CTAs per SM used by advance(),
+        and whether the 2nd and 3rd advance after an add/remove rebalance first."""
         L = _lib.lib()
+        if auto_balance is not None:
+            _lib.check(L.phs_engine_config(self._h, _lib.CFG_AUTO_BALANCE, int(bool(auto_balance))),
+                       "phs_engine_config")
         if variant is not None:
             _lib.check(L.phs_engine_config(self._h, _lib.CFG_VARIANT, int(variant)), "phs_engine_config")
         if ctas_per_sm is not None:
