@@ -464,6 +464,17 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     // ---- leader bodies ------------------------------------------------------
+    // statistics of a solve that iterated, recorded by the leader that ends it
+    auto account_solve = [&]() {
+        const int it = sc->iters_solve;
+        if (it > 0) {
+            I.st->arnoldi += it;
+            I.st->arnoldi_sq += (long long)it * it;
+            I.st->solves += 1;
+            if (it > I.st->max_arnoldi) I.st->max_arnoldi = it;
+        }
+    };
+
     auto leader_rhs = [&]() {
         __shared__ double s_r2;
         if (warp == 1) {
@@ -554,6 +565,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     sc->s[j + 1] = 1.0 / hn;
                 }
                 if (act == ACT_UPDATE_FINAL || act == ACT_UPDATE_CHECK) sc->k = j + 1;
+                if (act == ACT_UPDATE_FINAL) account_solve();
                 sc->action = act;
             }
         }
@@ -591,8 +603,10 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     I.st->status = PHS_ERR_NONFINITE;
                 } else if (rn <= sc->atol_eff) {
                     act = ACT_DONE;
+                    account_solve();
                 } else if (sc->iters_cap >= I.maxiter) {
                     act = ACT_DONE;
+                    account_solve();
                     I.st->nonconv += 1;
                     if (I.st->status == PHS_OK) I.st->status = PHS_WARN_NO_CONVERGE;
                 } else {
@@ -605,17 +619,6 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
     };
 
-    auto leader_solve_stats = [&]() {
-        if (threadIdx.x == 0) {
-            int it = sc->iters_solve;
-            if (it > 0) {
-                I.st->arnoldi += it;
-                I.st->arnoldi_sq += (long long)it * it;
-                I.st->solves += 1;
-                if (it > I.st->max_arnoldi) I.st->max_arnoldi = it;
-            }
-        }
-    };
 
     auto read_action = [&]() {
         if (threadIdx.x == 0) {
@@ -932,9 +935,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             break;
         }
         mark(PF_COPY);
-        // end of step: u visible to every CTA of the team; solve statistics
-        if (!team_sync(I.sync, P, abort_word, ctl, leader_solve_stats)) { aborted = true; break; }
-        mark(PF_STEP_WAIT);
+        // No barrier at the end of the step: each voxel's u and h are written and
+        // read again (next RHS pass 1) by the same thread, and every cross-CTA read
+        // of the next step follows its mid-RHS barrier.
         if (prof_on && threadIdx.x == 0) pf[PF_STEPS] += 1;
         hbuf ^= 1;
         const bool due = (I.stride > 0) ? (step % I.stride == 0) : true;
