@@ -362,6 +362,12 @@ __device__ __forceinline__ T edge_row(const T* vec, const int32_t* enb, const T*
     return acc;
 }
 
+// Bulk L2 prefetch of [p, p + bytes) (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
+    const unsigned long long g = (unsigned long long)__cvta_generic_to_global(p);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
+}
+
 constexpr int kChunk = 4;  // basis vectors whose loads are issued together
 template <typename T>
 constexpr bool kWarpParts = sizeof(T) == 4;
@@ -450,6 +456,34 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
     };
     auto voxel = [&](int tile, int v) -> long long { return (long long)tile * TILE + v * kThreads + threadIdx.x; };
+
+    // Prefetch into L2 the slice of an array (elem bytes per voxel) that `tile`
+    // will read, so that the loads of the CTA's next tile find it there.  Start
+    // and end are rounded down to 16 bytes: every prefetched byte lies inside
+    // the array (whose allocation starts 256-byte aligned).
+    auto pf_slice = [&](const void* arr, int elem, int tile) {
+        if (arr == nullptr || tile >= I.n_tiles) return;
+        const long long v0 = (long long)tile * TILE;
+        const long long v1 = (v0 + TILE < N) ? v0 + TILE : N;
+        uintptr_t a = reinterpret_cast<uintptr_t>(arr) + (uintptr_t)(v0 * elem);
+        uintptr_t b = reinterpret_cast<uintptr_t>(arr) + (uintptr_t)(v1 * elem);
+        a &= ~(uintptr_t)15;
+        b &= ~(uintptr_t)15;
+        if (b > a) prefetch_l2(reinterpret_cast<const void*>(a), (unsigned int)(b - a));
+    };
+    // the row tables of the operator (neighbours, coefficients, flags, edges)
+    auto pf_rows = [&](int t, int tile) {
+        switch (t) {
+            case 0: pf_slice(I.nb, 24, tile); break;
+            case 1: pf_slice(I.cw ? (const void*)I.cw : (const void*)I.coef, I.cw ? (int)sizeof(T) : 6 * (int)sizeof(T), tile); break;
+            case 2: pf_slice(I.m6, 1, tile); break;
+            case 3: pf_slice(I.vflags, 1, tile); break;
+            case 4: if (EDGE) pf_slice(I.enb, 48, tile); break;
+            case 5: if (EDGE) pf_slice(I.ecf, 6 * (int)sizeof(T), tile); break;
+            default: break;
+        }
+    };
+    constexpr int kRowArrays = 6;
 
     auto params_of = [&](long long n, T* p) {
         if (I.vparams) {
@@ -683,6 +717,13 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         // was 17 % slower over the batch.)
         T* Us = Vb + ldV;
         for (int tile = rank; tile < I.n_tiles; tile += P) {
+            if (threadIdx.x < 4) {
+                const int t = threadIdx.x;
+                if (t == 0) pf_slice(I.u, sizeof(T), tile + P);
+                else if (t == 1) pf_slice(hin, sizeof(T), tile + P);
+                else if (t == 2) pf_slice(I.vflags, 1, tile + P);
+                else pf_slice(I.vparams, 5 * sizeof(T), tile + P);
+            }
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
@@ -703,6 +744,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         pending = -1;
         if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
         for (int tile = rank; tile < I.n_tiles; tile += P) {
+            if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
+            else if (threadIdx.x == kRowArrays) pf_slice(Us, sizeof(T), tile + P);
+            else if (threadIdx.x == kRowArrays + 1) pf_slice(I.dx, sizeof(T), tile + P);
             double ab = 0.0, ar = 0.0;
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
@@ -762,6 +806,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     const T* Vj = Vb + (size_t)j * ldV;
                     T* Vn = Vb + (size_t)(j + 1) * ldV;
                     for (int tile = rank; tile < I.n_tiles; tile += P) {
+                        if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
+                        else if (threadIdx.x <= kRowArrays + j)
+                            pf_slice(Vb + (size_t)(threadIdx.x - kRowArrays) * ldV, sizeof(T), tile + P);
                         T wr[VPT];
 #pragma unroll
                         for (int v = 0; v < VPT; ++v) {
@@ -807,6 +854,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     mark(PF_A_WAIT);
                     // ============ phase C: u = w - sum_i c_i V_i  (in place), ||u||^2
                     for (int tile = rank; tile < I.n_tiles; tile += P) {
+                        if (threadIdx.x <= j + 1) pf_slice(Vb + (size_t)threadIdx.x * ldV, sizeof(T), tile + P);
                         double acc[VPT];
 #pragma unroll
                         for (int v = 0; v < VPT; ++v) {
@@ -861,6 +909,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 load_shc(k);
                 const bool final = (act == ACT_UPDATE_FINAL);
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
+                    if (threadIdx.x < k) pf_slice(Vb + (size_t)threadIdx.x * ldV, sizeof(T), tile + P);
+                    else if (threadIdx.x == k) pf_slice(I.x, sizeof(T), tile + P);
+                    else if (threadIdx.x == k + 1 && final) pf_slice(I.dx, sizeof(T), tile + P);
                     double acc[VPT], x_in[VPT];
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
@@ -888,6 +939,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 // ============ true residual of the new iterate (start of the next cycle)
                 if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
+                    if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
+                    else if (threadIdx.x == kRowArrays) pf_slice(I.x, sizeof(T), tile + P);
+                    else if (threadIdx.x == kRowArrays + 1) pf_slice(I.b, sizeof(T), tile + P);
                     double a2 = 0.0;
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
@@ -924,6 +978,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         } else if (act == ACT_ZERO_B || act == ACT_DONE) {
             const T* src = (act == ACT_ZERO_B) ? I.b : I.x;
             for (int tile = rank; tile < I.n_tiles; tile += P) {
+                if (threadIdx.x == 0) pf_slice(src, sizeof(T), tile + P);
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
                     const long long n = voxel(tile, v);
