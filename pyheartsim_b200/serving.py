@@ -70,7 +70,10 @@ def footprint_bytes(inst):
     n = inst.n_voxel
     m = min(inst.restart, n)
     tiles = math.ceil(n / 1024)
-    per_voxel = 24 + 24 + 1 + 5 * 4 + (m + 1) * 4 + 4 + inst.n_samples * 4 * (2 if inst.save_h else 1)
+    cb = 5 if getattr(inst, "cw", None) is not None else 24
+    eb = 72 if getattr(inst, "coef_edge", None) is not None else 0
+    per_voxel = (24 + cb + eb + 1 + 5 * 4 + (m + 1) * 4 + 4 + (4 if inst.guess else 0)
+                 + inst.n_samples * 4 * (2 if inst.save_h else 1))
     return n * per_voxel + tiles * 8 * (m + 2) * 8 + inst.n_steps + 64 * 1024
 
 
