@@ -280,23 +280,6 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
     return ctl.abort == 0;
 }
 
-// Leader helper: sum one partial slot over every (tile, warp) of the instance in
-// (tile, warp) order.  Lane l sums entries l, l+32, ... and the lanes combine in
-// a fixed xor tree, so the result does not depend on which CTA processed which
-// tile.  Called by one warp; returns the sum in every lane.
-__device__ __forceinline__ double tile_sum(const double* part, int count, int ps, int slot) {
-    const int lane = threadIdx.x & 31;
-    double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    int q = lane;
-    for (; q + 7 * 32 < count; q += 8 * 32) {
-#pragma unroll
-        for (int u = 0; u < 8; ++u) a[u] += __ldcg(part + (size_t)(q + 32 * u) * ps + slot);
-    }
-    for (; q < count; q += 32) a[0] += __ldcg(part + (size_t)q * ps + slot);
-    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-    return warp_sum(s);
-}
-
 // The six (neighbour, coefficient) pairs of row n, as 8/16-byte vector loads.
 __device__ __forceinline__ void load_nb(const int32_t* nb, long long n, int32_t (&q)[6]) {
     const int2* p = reinterpret_cast<const int2*>(nb + 6 * n);
@@ -498,6 +481,39 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     // ---- leader bodies ------------------------------------------------------
+    // Deterministic sums of partial slots slot0 .. slot0+ns-1 over all tiles, by
+    // the whole leader CTA: thread t adds partials t, t+256, ... in order (four
+    // slots per pass, their loads issued together), then a fixed xor tree per
+    // warp and the warp results in warp order.  The order depends only on the
+    // partial count, not on the team size.  Results in bsum_out[0..ns).
+    __shared__ double bsum_w[kMaxRestart + 1][kWarps];
+    __shared__ double bsum_out[kMaxRestart + 1];
+    auto block_sum = [&](int slot0, int ns) {
+        for (int s0 = 0; s0 < ns; s0 += 4) {
+            double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+            for (int q = threadIdx.x; q < nparts; q += kThreads) {
+                const double* pq = I.part + (size_t)q * ps + slot0 + s0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (s0 + u < ns) a[u] += __ldcg(pq + u);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double v = warp_sum(a[u]);
+                if (lane == 0 && s0 + u < ns) bsum_w[s0 + u][warp] = v;
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < ns; i += kThreads) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < kWarps; ++w) t += bsum_w[i][w];
+            bsum_out[i] = t;
+        }
+        __syncthreads();
+    };
+
     // statistics of a solve that iterated, recorded by the leader that ends it
     auto account_solve = [&]() {
         const int it = sc->iters_solve;
@@ -510,15 +526,10 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     auto leader_rhs = [&]() {
-        __shared__ double s_r2;
-        if (warp == 1) {
-            double r2 = tile_sum(I.part, nparts, ps, 1);
-            if (lane == 0) s_r2 = r2;
-        }
-        __syncthreads();
+        block_sum(0, 2);
         if (warp == 0) {
-            double b2 = tile_sum(I.part, nparts, ps, 0);
-            double r2 = s_r2;
+            double b2 = bsum_out[0];
+            double r2 = bsum_out[1];
             if (lane == 0) {
                 double bn = sqrt(b2), rn = sqrt(r2);
                 double atol_eff = fmax(I.atol, I.tol * bn);
@@ -544,20 +555,19 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     auto leader_dots = [&](int j) {
         // h_ij = s_i * sum <V_i, w>;  published coef_i = h_ij * s_i
-        for (int i = warp; i <= j; i += kWarps) {
-            double d = tile_sum(I.part, nparts, ps, i);
-            if (lane == 0) {
-                double si = sc->s[i];
-                double h = si * d;
-                sc->R[j * (kMaxRestart + 1) + i] = h;
-                sc->coef[i] = h * si;
-            }
+        block_sum(0, j + 1);
+        for (int i = threadIdx.x; i <= j; i += kThreads) {
+            double si = sc->s[i];
+            double h = si * bsum_out[i];
+            sc->R[j * (kMaxRestart + 1) + i] = h;
+            sc->coef[i] = h * si;
         }
     };
 
     auto leader_norm = [&](int j) {
+        block_sum(0, 1);
         if (warp == 0) {
-            double u2 = tile_sum(I.part, nparts, ps, 0);
+            double u2 = bsum_out[0];
             if (lane == 0) {
                 double* Rc = sc->R + j * (kMaxRestart + 1);
                 double hn = sqrt(u2);
@@ -625,8 +635,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     auto leader_check = [&]() {
+        block_sum(0, 1);
         if (warp == 0) {
-            double r2 = tile_sum(I.part, nparts, ps, 0);
+            double r2 = bsum_out[0];
             if (lane == 0) {
                 double rn = sqrt(r2);
                 sc->rnorm = rn;
