@@ -327,7 +327,7 @@ def phase_profile(eng, slots, S, stream):
         team = p.pop("team_ctas")
         inst = eng.instance(s)
         per.append([int(inst.n_voxel), int(inst.model), int(team), round(it / st, 2),
-                    round(sum(p.values()) / st, 4), round(p["rhs"] / st, 4)])
+                    round(sum(p.values()) / st, 4), round(p["rhs_reaction"] / st, 4), round(p["rhs"] / st, 4)])
         for k, v in p.items():
             acc[k] = acc.get(k, 0.0) + v / st
         acc["arnoldi_iters_per_step"] = acc.get("arnoldi_iters_per_step", 0.0) + it / st

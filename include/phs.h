@@ -165,9 +165,10 @@ int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, i
  * step).  Synchronises the device; the next advance() rebuilds its plan.        */
 int phs_engine_rebalance(phs_engine* eng);
 /* Phase timers of an instance (PHS_CFG_PROFILE on): 16 counters, nanoseconds
- * spent by the team's first CTA in [0] RHS, [1] its barrier, [2] Arnoldi phase A,
- * [3] its barrier, [4] phase C, [5] its barrier, [6] update, [7] residual check,
- * [8] its barrier, [9] final copy, [10] end-of-step barrier; [11] steps and
+ * spent by the team's first CTA in [0] RHS pass 2 (right-hand side, initial
+ * residual), [1] the RHS barriers, [2] Arnoldi phase A, [3] its barrier, [4]
+ * phase C, [5] its barrier, [6] update, [7] residual check, [8] its barrier,
+ * [9] final copy, [10] RHS pass 1 (reaction); [11] steps and
  * [12] Arnoldi iterations counted; [13] CTAs in the team at the last launch.   */
 int phs_instance_profile(phs_engine* eng, int slot, uint64_t* out16);
 

@@ -35,7 +35,7 @@ CFG_PROFILE = 3
 CFG_TEST_TEAM_OVERCOUNT = 4
 CFG_AUTO_BALANCE = 5
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
-                 "check", "check_wait", "copy", "step_wait", "steps", "arnoldi_iters", "team_ctas")
+                 "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas")
 
 VFLAG_S1 = 1
 VFLAG_S2 = 2

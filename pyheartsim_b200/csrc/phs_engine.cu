@@ -62,7 +62,7 @@ enum Phase : int { PH_PLAIN = 0, PH_RHS = 1, PH_DOTS = 2, PH_NORM = 3, PH_CHECK 
 // Phase timer slots (nanoseconds of globaltimer, summed over steps).
 enum ProfSlot : int {
     PF_RHS = 0, PF_RHS_WAIT, PF_A, PF_A_WAIT, PF_C, PF_C_WAIT, PF_X, PF_CHECK, PF_CHECK_WAIT,
-    PF_COPY, PF_STEP_WAIT, PF_STEPS, PF_SOLVE_ITERS, PF_TEAM, kProfSlots = 16
+    PF_COPY, PF_RHS1, PF_STEPS, PF_SOLVE_ITERS, PF_TEAM, kProfSlots = 16
 };
 
 struct Scalars {
@@ -753,7 +753,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             }
         }
         pending = -1;
+        mark(PF_RHS1);
         if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+        mark(PF_RHS_WAIT);
         for (int tile = rank; tile < I.n_tiles; tile += P) {
             if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
             else if (threadIdx.x == kRowArrays) pf_slice(Us, sizeof(T), tile + P);
@@ -1754,7 +1756,7 @@ int phs_engine_rebalance(phs_engine* e) {
             PHS_CUDA_TRY(cudaMemcpy(pf, h.prof, sizeof(pf), cudaMemcpyDeviceToHost));
             const unsigned long long steps = pf[PF_STEPS] - h.prof_ref[PF_STEPS];
             unsigned long long ns = 0;
-            for (int i = 0; i <= PF_STEP_WAIT; ++i) ns += pf[i] - h.prof_ref[i];
+            for (int i = 0; i <= PF_RHS1; ++i) ns += pf[i] - h.prof_ref[i];
             if (steps > 0 && h.team > 0) h.weight = (double)ns / (double)steps * (double)h.team;
             for (int i = 0; i < kProfSlots; ++i) h.prof_ref[i] = pf[i];
         }
