@@ -31,11 +31,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
 # DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, median of 24 full-size launches of this batch at 2.40
-# Arnoldi steps per solve, profiles/step_kernel_64shells_dram_fullsize.md);
+# dram__bytes_write.sum, median of 24 full-size launches of this batch at 2.05
+# Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md);
 # multiplied by the voxels and steps of one launch below.
-STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 219.5
-STEP_TRAFFIC_ARNOLDI_PER_SOLVE = 2.40
+STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 232.4
+STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.05
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
 
 
@@ -277,7 +277,8 @@ def run_b200(args):
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
                          "traffic": STEP_TRAFFIC_BYTES_PER_VOXEL_STEP * float(ns.sum()) * S,
                          "traffic_source": ("ncu dram__bytes_read+write per voxel-step of full-size launches of this "
-                                            f"batch (k={STEP_TRAFFIC_ARNOLDI_PER_SOLVE}) x voxels x steps per launch"),
+                                            f"batch ({STEP_TRAFFIC_ARNOLDI_PER_STEP} Arnoldi steps per step) x voxels "
+                                            "x steps per launch"),
                          "kernel": step_kernel_name(tune),
                          "bytes_per_voxel_step": alg_bytes / local_vs},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
