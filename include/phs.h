@@ -98,6 +98,10 @@ typedef struct phs_instance_desc {
      * a = nb_edge[n][2p], b = nb_edge[n][2p+1].  Both NULL for D0 = I.          */
     const int32_t* nb_edge;   /* [n][12] edge neighbours (a0,b0,...,a5,b5), absent -> 0     */
     const double* coef_edge;  /* [n][6]  c_n/(4 Delta^2) * P_2d[n,9+p]                      */
+    int32_t device_tables;    /* 1: nb6, coef6, cw, mask6, vflags, vparams, nb_edge and
+                                 coef_edge are device pointers (built by phs_operator_tables;
+                                 checked on the device); stim stays on the host            */
+    int32_t _pad;
 } phs_instance_desc;
 
 /* Per-instance progress and solver statistics. */
@@ -232,6 +236,65 @@ int phs_electrogram(int64_t T, int64_t n_v, int64_t n_e, const double* V, const 
                     const double* electrode_xyz, const double* c_voxel, const double* D0,
                     const int32_t* in_ptr, const int32_t* in_src, const int8_t* in_dir,
                     double delta, int mode, double* egm_out);
+
+/* ------------------------------------------------ geometry on the device
+ * The inputs of the time stepper built on the GPU from lattice coordinates.
+ * Replaces the host loops of utility/voxelization.py:102-152
+ * (find_neighbor_voxel_ids), simulation/equation_parts.py:36-114
+ * (heart_model_equation_parts) and the table build of
+ * simulation/simulation_gpu.py:138-225 / 294-330.  Array arguments are device
+ * pointers; each call is ordered on `stream` and returns once it has drained. */
+
+/* Neighbour table nb18 [n][18] of integer lattice coordinates ijk [n][3], in the
+ * reference's column order with -1 for an absent neighbour.  order (may be NULL)
+ * receives the voxels sorted by (z, y, x), x fastest: order[r] = voxel of rank r.
+ * PHS_ERR_BAD_TABLE: two voxels share coordinates; PHS_ERR_UNSUPPORTED: the
+ * bounding box exceeds 2^31 cells.  Works in a temporary dense grid over the box. */
+int phs_lattice_neighbors(int64_t n, const int32_t* ijk, int32_t* nb18, int32_t* order, void* stream);
+
+/* P_2d [n][21] (FP64), bit-identical to the reference, from nb18, D0 [n][3][3]
+ * (NULL: identity, the reference's load_fiber) and par [n][6] = P_2d columns
+ * 15..20 (five model parameters, then c). */
+int phs_equation_parts(int64_t n, const int32_t* nb18, const double* D0, const double* par, double* P,
+                       void* stream);
+
+/* out3 (host): [0] some face cross term P_2d[:,6..8] is non-zero, [1] some edge
+ * cross term P_2d[:,9..14] is non-zero, [2] P_2d[:,15..19] is the same on every row. */
+int phs_operator_flags(int64_t n, const double* P, int32_t* out3, void* stream);
+
+/* Operator tables of one instance in device row order, as the host compilation
+ * builds them (face neighbours remapped -1 -> 0 and through the order, the
+ * coefficients c/(4 Delta^2) P_2d[:,k] with the face cross terms folded in when
+ * face_cross is set, the isotropic row form, S1/S2/temporary-block flags,
+ * per-voxel parameters, edge pairs when edge is set).                        */
+typedef struct phs_operator_tables_args {
+    int64_t n_voxel;
+    double Delta;
+    const double* P;          /* [n][21], caller order                                      */
+    const int32_t* nb18;      /* [n][18], caller order, -1 absent                           */
+    const int32_t* node_flag; /* [n] or NULL: 4 permanent block (c -> 0), 3 temporary block */
+    const int32_t* order;     /* [n]: device row r holds caller voxel order[r]; NULL = same */
+    int32_t* inv;             /* [n] out: device row of each caller voxel                   */
+    int32_t* nb6;             /* [n][6] out                                                 */
+    double* coef6;            /* [n][6] out                                                 */
+    double* cw;               /* [n] out: first non-zero coefficient of the row (or 0)      */
+    uint8_t* mask6;           /* [n] out: bit k set when coefficient k is non-zero          */
+    uint8_t* vflags;          /* [n] out: PHS_VFLAG_* bits                                  */
+    double* vparams;          /* [n][5] out: P_2d[:,15..19], or NULL to skip                */
+    int32_t* nb_edge;         /* [n][12] out when edge != 0                                 */
+    double* coef_edge;        /* [n][6] out when edge != 0                                  */
+    const int64_t* s1;        /* [n_s1] caller ids of the S1 pacing set, or NULL            */
+    int64_t n_s1;
+    const int64_t* s2;        /* [n_s2] caller ids of the S2 pacing set, or NULL            */
+    int64_t n_s2;
+    uint32_t* iso_word;       /* device workspace, one word                                 */
+    int32_t face_cross;       /* in: from phs_operator_flags                                */
+    int32_t edge;             /* in: from phs_operator_flags                                */
+    int32_t iso;              /* out: every row is isotropic (cw, mask6 describe it)        */
+    int32_t _pad;
+    void* stream;
+} phs_operator_tables_args;
+int phs_operator_tables(phs_operator_tables_args* args);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,39 @@ class InstanceDesc(ctypes.Structure):
         ("mask6", c_uint8_p),
         ("nb_edge", c_int32_p),
         ("coef_edge", c_double_p),
+        ("device_tables", ctypes.c_int32),
+        ("_pad", ctypes.c_int32),
+    ]
+
+
+class OperatorTablesArgs(ctypes.Structure):
+    """Mirror of ``phs_operator_tables_args`` (device pointers as void*)."""
+    _fields_ = [
+        ("n_voxel", ctypes.c_int64),
+        ("Delta", ctypes.c_double),
+        ("P", ctypes.c_void_p),
+        ("nb18", ctypes.c_void_p),
+        ("node_flag", ctypes.c_void_p),
+        ("order", ctypes.c_void_p),
+        ("inv", ctypes.c_void_p),
+        ("nb6", ctypes.c_void_p),
+        ("coef6", ctypes.c_void_p),
+        ("cw", ctypes.c_void_p),
+        ("mask6", ctypes.c_void_p),
+        ("vflags", ctypes.c_void_p),
+        ("vparams", ctypes.c_void_p),
+        ("nb_edge", ctypes.c_void_p),
+        ("coef_edge", ctypes.c_void_p),
+        ("s1", ctypes.c_void_p),
+        ("n_s1", ctypes.c_int64),
+        ("s2", ctypes.c_void_p),
+        ("n_s2", ctypes.c_int64),
+        ("iso_word", ctypes.c_void_p),
+        ("face_cross", ctypes.c_int32),
+        ("edge", ctypes.c_int32),
+        ("iso", ctypes.c_int32),
+        ("_pad", ctypes.c_int32),
+        ("stream", ctypes.c_void_p),
     ]
 
 
@@ -144,6 +177,12 @@ SIGNATURES = {
     "phs_electrogram": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, c_double_p, c_double_p,
                                        c_double_p, c_double_p, c_double_p, c_int32_p, c_int32_p, c_int8_p,
                                        ctypes.c_double, ctypes.c_int, c_double_p]),
+    "phs_lattice_neighbors": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p]),
+    "phs_equation_parts": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_operator_flags": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, c_int32_p, ctypes.c_void_p]),
+    "phs_operator_tables": (ctypes.c_int, [ctypes.POINTER(OperatorTablesArgs)]),
 }
 
 _lib = None

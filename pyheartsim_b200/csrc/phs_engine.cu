@@ -1187,22 +1187,46 @@ void fill_dev(T* p, long long n, T v, cudaStream_t s) {
     fill_kernel<T><<<(unsigned)blocks, 256, 0, s>>>(p, n, v);
 }
 
+// Device-side form of validate_desc's table checks (device_tables instances).
 template <typename T>
-int upload_converted(void** dst, const double* src, long long n) {
+__global__ void check_tables(long long n, const int32_t* nb, const T* coef, const T* cw, const uint8_t* m6,
+                             const int32_t* enb, const T* ecf, unsigned int* err) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
+        bool bad = false;
+        for (int k = 0; k < 6; ++k) {
+            const int32_t q = nb[6 * r + k];
+            bad |= (q < 0 || q >= n);
+            if (coef) bad |= !isfinite((double)coef[6 * r + k]);
+        }
+        if (cw) bad |= !isfinite((double)cw[r]) || (m6[r] & 0xC0u);
+        if (enb) {
+            for (int k = 0; k < 12; ++k) bad |= (enb[12 * r + k] < 0 || enb[12 * r + k] >= n);
+            for (int k = 0; k < 6; ++k) bad |= !isfinite((double)ecf[6 * r + k]);
+        }
+        if (bad) atomicOr(err, 1u);
+    }
+}
+
+// Copy n doubles (host, or device when on_device) into a new array of T.
+template <typename T>
+int upload_converted(void** dst, const double* src, long long n, bool on_device = false) {
     PHS_CUDA_TRY(cudaMalloc(dst, (size_t)n * sizeof(T)));
     if (sizeof(T) == 8) {
-        PHS_CUDA_TRY(cudaMemcpy(*dst, src, (size_t)n * 8, cudaMemcpyHostToDevice));
+        PHS_CUDA_TRY(cudaMemcpy(*dst, src, (size_t)n * 8, cudaMemcpyDefault));
         return PHS_OK;
     }
     double* tmp = nullptr;
-    PHS_CUDA_TRY(cudaMalloc(&tmp, (size_t)n * 8));
-    cudaError_t e = cudaMemcpy(tmp, src, (size_t)n * 8, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaSuccess;
+    if (!on_device) {
+        PHS_CUDA_TRY(cudaMalloc(&tmp, (size_t)n * 8));
+        e = cudaMemcpy(tmp, src, (size_t)n * 8, cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) {
         long long blocks = std::min<long long>((n + 255) / 256, 65535);
-        convert_kernel<T><<<(unsigned)std::max<long long>(blocks, 1), 256>>>(tmp, (T*)*dst, n);
+        convert_kernel<T><<<(unsigned)std::max<long long>(blocks, 1), 256>>>(on_device ? src : tmp, (T*)*dst, n);
         e = cudaDeviceSynchronize();
     }
-    cudaFree(tmp);
+    if (tmp) cudaFree(tmp);
     if (e != cudaSuccess) { set_last_error("upload_converted", e); return PHS_ERR_CUDA; }
     return PHS_OK;
 }
@@ -1216,6 +1240,8 @@ int validate_desc(const phs_instance_desc* d) {
     if (d->n_steps < 0 || (d->n_steps > 0 && !d->stim)) return PHS_ERR_BAD_ARG;
     if (d->n_samples < 0 || d->sample_stride < 0 || d->maxiter < 1) return PHS_ERR_BAD_ARG;
     if (!(d->dt > 0.0)) return PHS_ERR_BAD_ARG;
+    if ((d->nb_edge == nullptr) != (d->coef_edge == nullptr)) return PHS_ERR_BAD_ARG;
+    if (d->device_tables) return PHS_OK;   // checked on the device after the copy (check_tables)
     const long long n = d->n_voxel;
     for (long long i = 0; i < 6 * n; ++i) {
         int32_t q = d->nb6[i];
@@ -1225,7 +1251,6 @@ int validate_desc(const phs_instance_desc* d) {
     if (d->cw)
         for (long long i = 0; i < n; ++i)
             if (!std::isfinite(d->cw[i]) || (d->mask6[i] & 0xC0u)) return PHS_ERR_BAD_TABLE;
-    if ((d->nb_edge == nullptr) != (d->coef_edge == nullptr)) return PHS_ERR_BAD_ARG;
     if (d->nb_edge) {
         for (long long i = 0; i < 12 * n; ++i)
             if (d->nb_edge[i] < 0 || d->nb_edge[i] >= n) return PHS_ERR_BAD_TABLE;
@@ -1254,25 +1279,45 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
         cudaError_t _e = cudaMalloc((void**)&(ptr), (bytes));            \
         if (_e != cudaSuccess) { set_last_error("cudaMalloc", _e); return fail(PHS_ERR_OOM); } \
     } while (0)
+    // tables: host arrays, or device arrays when device_tables (cudaMemcpyDefault)
+    const bool dev = d->device_tables != 0;
     PHS_ALLOC(h.nb, n * 6 * sizeof(int32_t));
-    if (cudaMemcpy(h.nb, d->nb6, n * 6 * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
+    if (cudaMemcpy(h.nb, d->nb6, n * 6 * sizeof(int32_t), cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
     if (d->cw) {
-        if ((rc = upload_converted<T>(&h.cw, d->cw, (long long)n)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.cw, d->cw, (long long)n, dev)) != PHS_OK) return fail(rc);
         PHS_ALLOC(h.m6, n);
-        if (cudaMemcpy(h.m6, d->mask6, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
+        if (cudaMemcpy(h.m6, d->mask6, n, cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
     } else {
-        if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6, dev)) != PHS_OK) return fail(rc);
     }
     if (d->nb_edge) {
         PHS_ALLOC(h.enb, n * 12 * sizeof(int32_t));
-        if (cudaMemcpy(h.enb, d->nb_edge, n * 12 * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess)
+        if (cudaMemcpy(h.enb, d->nb_edge, n * 12 * sizeof(int32_t), cudaMemcpyDefault) != cudaSuccess)
             return fail(PHS_ERR_CUDA);
-        if ((rc = upload_converted<T>(&h.ecf, d->coef_edge, (long long)n * 6)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.ecf, d->coef_edge, (long long)n * 6, dev)) != PHS_OK) return fail(rc);
     }
     PHS_ALLOC(h.vflags, n);
-    if (cudaMemcpy(h.vflags, d->vflags, n, cudaMemcpyHostToDevice) != cudaSuccess) return fail(PHS_ERR_CUDA);
+    if (cudaMemcpy(h.vflags, d->vflags, n, cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
     if (d->vparams) {
-        if ((rc = upload_converted<T>(&h.vparams, d->vparams, (long long)n * 5)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.vparams, d->vparams, (long long)n * 5, dev)) != PHS_OK) return fail(rc);
+    }
+    if (dev) {
+        // the checks validate_desc makes on host tables, on the copies
+        unsigned int* d_err = nullptr;
+        if (cudaMalloc((void**)&d_err, sizeof(unsigned int)) != cudaSuccess) return fail(PHS_ERR_OOM);
+        unsigned int h_err = 0;
+        cudaError_t ce = cudaMemset(d_err, 0, sizeof(unsigned int));
+        if (ce == cudaSuccess) {
+            const long long blocks = std::max<long long>(1, std::min<long long>(((long long)n + 255) / 256, 65535));
+            check_tables<T><<<(unsigned)blocks, 256>>>((long long)n, (const int32_t*)h.nb, (const T*)h.coef,
+                                                       (const T*)h.cw, (const uint8_t*)h.m6, (const int32_t*)h.enb,
+                                                       (const T*)h.ecf, d_err);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpy(&h_err, d_err, sizeof(h_err), cudaMemcpyDeviceToHost);
+        cudaFree(d_err);
+        if (ce != cudaSuccess) { set_last_error("check_tables", ce); return fail(PHS_ERR_CUDA); }
+        if (h_err) return fail(PHS_ERR_BAD_TABLE);
     }
     const size_t ns = (size_t)std::max<int64_t>(d->n_steps, 1);
     PHS_ALLOC(h.stim, ns);

@@ -152,6 +152,32 @@ def tblock_steps(n_steps, dt):
     return k
 
 
+def instance_scalars(simulation_parameters, arrhythmia_parameters, *, full_cycles=True, tol=1e-5, atol=1e-5,
+                     restart=50, maxiter=10000, pacing_duration=None, save_h=True, max_steps=None, guess=None):
+    """The per-instance scalars and the pacing schedule (everything but the
+    per-voxel tables), and the S1 / S2 voxel ids (caller order, int64)."""
+    model = int(simulation_parameters['heart_model_flag'])
+    if model not in (0, 1):
+        raise ValueError("heart_model_flag must be 0 (Mitchell-Schaeffer) or 1 (Aliev-Panfilov)")
+    flag = simulation_parameters['arrhythmia_flag']
+    dt = simulation_parameters['dt']
+    n_steps, n_samples, stride = step_counts(simulation_parameters)
+    if max_steps is not None:
+        n_steps = min(n_steps, int(max_steps))
+    s1, s2, s1_t, jmag, pdur, s2_t = pacing.assign_pacing_parameters(
+        arrhythmia_parameters, flag, simulation_parameters, pacing_duration)
+    stim = pacing.schedule(n_steps, dt, arrhythmia_parameters, simulation_parameters, flag, s1_t, pdur, s2_t)
+    s1 = np.atleast_1d(np.asarray(s1, dtype=np.int64)) if np.size(s1) else np.zeros(0, np.int64)
+    s2 = np.atleast_1d(np.asarray(s2, dtype=np.int64)) if np.size(s2) else np.zeros(0, np.int64)
+    u0, h0 = (0.0, 1.0) if model == 0 else (0.0, 0.0)
+    sc = dict(model=model, restart=int(min(restart, 50)), dt=float(dt), j_stim=float(jmag), n_steps=int(n_steps),
+              stim=np.ascontiguousarray(stim, dtype=np.uint8), sample_stride=int(stride), n_samples=int(n_samples),
+              save_h=int(bool(save_h)), full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol),
+              atol=float(atol), maxiter=int(maxiter), time_scale=simulation_parameters['time_scale'],
+              guess=int((not full_cycles) if guess is None else bool(guess)))
+    return sc, s1, s2
+
+
 def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
                      full_cycles=True, tol=1e-5, atol=1e-5, restart=50, maxiter=10000,
                      pacing_duration=None, save_h=True, max_steps=None, reorder="rows", guess=None):
@@ -180,20 +206,10 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
     if cross_edge and (nb.shape[1] < 18 or np.any(nb[:, 6:18] < -1) or np.any(nb[:, 6:18] >= n)):
         raise ValueError("edge cross terms need neighbor_id_2d columns 6..17 in [-1, n_voxel)")
     Delta = float(geometry_data['Delta'])
-    model = int(simulation_parameters['heart_model_flag'])
-    if model not in (0, 1):
-        raise ValueError("heart_model_flag must be 0 (Mitchell-Schaeffer) or 1 (Aliev-Panfilov)")
-    flag = simulation_parameters['arrhythmia_flag']
-    dt = simulation_parameters['dt']
-    ts = simulation_parameters['time_scale']
+    sc, s1, s2 = instance_scalars(simulation_parameters, arrhythmia_parameters, full_cycles=full_cycles, tol=tol,
+                                  atol=atol, restart=restart, maxiter=maxiter, pacing_duration=pacing_duration,
+                                  save_h=save_h, max_steps=max_steps, guess=guess)
     node_flag = np.asarray(arrhythmia_parameters['node_flag'])
-
-    n_steps, n_samples, stride = step_counts(simulation_parameters)
-    if max_steps is not None:
-        n_steps = min(n_steps, int(max_steps))
-    s1, s2, s1_t, jmag, pdur, s2_t = pacing.assign_pacing_parameters(
-        arrhythmia_parameters, flag, simulation_parameters, pacing_duration)
-    stim = pacing.schedule(n_steps, dt, arrhythmia_parameters, simulation_parameters, flag, s1_t, pdur, s2_t)
 
     c = P[:, 20].copy()
     c[node_flag == 4] = 0.0                       # permanent block
@@ -211,12 +227,9 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         nb_edge[nb_edge == -1] = 0
         coef_edge = Dc[:, None] * P[:, pairs[:, 2]]
     vflags = np.zeros(n, dtype=np.uint8)
-    s1 = np.atleast_1d(np.asarray(s1, dtype=np.int64)) if np.size(s1) else np.zeros(0, np.int64)
-    s2 = np.atleast_1d(np.asarray(s2, dtype=np.int64)) if np.size(s2) else np.zeros(0, np.int64)
     vflags[s1] |= _lib.VFLAG_S1
     vflags[s2] |= _lib.VFLAG_S2
     vflags[node_flag == 3] |= _lib.VFLAG_TBLOCK
-    tb = tblock_steps(n_steps, dt) if np.any(node_flag == 3) else 0
 
     mp = P[:, 15:20]
     uniform = bool(np.all(mp == mp[0:1]))
@@ -245,15 +258,11 @@ def compile_instance(n_voxel, P_2d, geometry_data, simulation_parameters, arrhyt
         if nb_edge is not None:
             nb_edge = inv[nb_edge[order]]
             coef_edge = coef_edge[order]
-    u0, h0 = (0.0, 1.0) if model == 0 else (0.0, 0.0)
+    sc["tblock_steps"] = tblock_steps(sc["n_steps"], sc["dt"]) if np.any(node_flag == 3) else 0
     return CompiledInstance(
-        n_voxel=n, model=model, restart=int(min(restart, 50)), nb6=np.ascontiguousarray(nb6, dtype=np.int32),
-        coef6=np.ascontiguousarray(coef6), vflags=vflags, vparams=vparams, params=params, dt=float(dt),
-        j_stim=float(jmag), n_steps=int(n_steps), stim=np.ascontiguousarray(stim, dtype=np.uint8),
-        tblock_steps=int(tb), sample_stride=int(stride), n_samples=int(n_samples), save_h=int(bool(save_h)),
-        full_cycles=int(bool(full_cycles)), u0=u0, h0=h0, tol=float(tol), atol=float(atol),
-        maxiter=int(maxiter), time_scale=ts, Delta=Delta, order=order, inv=inv,
-        guess=int((not full_cycles) if guess is None else bool(guess)),
+        n_voxel=n, nb6=np.ascontiguousarray(nb6, dtype=np.int32),
+        coef6=np.ascontiguousarray(coef6), vflags=vflags, vparams=vparams, params=params,
+        Delta=Delta, order=order, inv=inv, **sc,
         cw=None if cw is None else np.ascontiguousarray(cw), mask6=None if mask6 is None else np.ascontiguousarray(mask6),
         nb_edge=None if nb_edge is None else np.ascontiguousarray(nb_edge, dtype=np.int32),
         coef_edge=None if coef_edge is None else np.ascontiguousarray(coef_edge))

@@ -33,8 +33,9 @@ def test_bindings_cover_header():
 
 def test_struct_layouts_match_c():
     # sizes fixed by include/phs.h (natural alignment, 64-bit)
-    assert ctypes.sizeof(_lib.InstanceDesc) == 216
+    assert ctypes.sizeof(_lib.InstanceDesc) == 224
     assert ctypes.sizeof(_lib.InstanceInfo) == 64
+    assert ctypes.sizeof(_lib.OperatorTablesArgs) == 184
 
 
 def test_status_strings_without_gpu():
