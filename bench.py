@@ -64,6 +64,7 @@ def parse():
     p.add_argument("--egm-only", action="store_true", help="run only the electrogram leg (profiling case)")
     p.add_argument("--aniso-only", action="store_true", help="run only the anisotropic (fibre) leg")
     p.add_argument("--aniso-instances", type=int, default=16)
+    p.add_argument("--geometry-only", action="store_true", help="run only the geometry-preparation leg")
     return p.parse_args()
 
 
@@ -290,6 +291,7 @@ def run_b200(args):
             line["plain_fp64"] = plain_leg(args, batch, value, dev)
             line["accuracy"] = accuracy_leg(dev, args.tol)
             line["anisotropic"] = aniso_leg(args, dev, tune, count=args.aniso_instances)
+            line["geometry"] = geometry_leg(args, dev)
             del batch, insts
             line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
             line["electrogram"] = egm_leg(args, dev)
@@ -404,6 +406,55 @@ def plain_leg(args, batch, fast_value, dev):
             "speedup_batched_fp32": fast_value / v}
 
 
+def geometry_leg(args, dev, n_target=1_000_000, reps=3):
+    """Instance preparation for one seeded ~1M-voxel scarred fibre shell: the
+    host path (vectorised numpy neighbour table, P_2d and table compilation)
+    against the device path (phs_lattice_neighbors, phs_equation_parts,
+    phs_operator_tables, instance add from device tables).  Wall time with the
+    device synchronised; the device path's best of ``reps``."""
+    import torch
+    from pyheartsim_b200 import _lib, geometry, geometry_gpu, instance, synthetic
+    from pyheartsim_b200.engine import BatchedEngine
+    ijk = synthetic.shell_for_size(n_target, seed=args.seed + 5)
+    n = ijk.shape[0]
+    rng = np.random.default_rng(args.seed)
+    c_scale = synthetic.scar(ijk, geometry.lattice_neighbors(ijk), 0.15, rng)
+    D0 = synthetic.fibre_tensors(ijk)
+    par = synthetic.model_parameters(0, n, np.full(n, 1.0) * c_scale)
+    sp = {'t_final': 100.0, 'dt': 0.05, 'heart_model_flag': 0, 'arrhythmia_flag': 4, 'time_scale': 1}
+    ap = {'pacing_start_time': 10.0, 'pacing_cycle_length': 300.0, 's1_pacing_voxel_id': np.arange(20),
+          's2_pacing_voxel_id': np.zeros(0, np.int64), 's1_t': 0.0, 's1_s2_delta_t': 0.0,
+          'node_flag': np.zeros(n, dtype=np.int64)}
+    kw = dict(full_cycles=False, tol=1e-7, restart=20, pacing_duration=2.0)
+    voxel = ijk * 0.4
+    t0 = time.perf_counter()
+    nb = geometry.lattice_neighbors(ijk)
+    P = geometry.heart_model_equation_parts(sp, n, D0, nb, par)
+    host = instance.compile_instance(n, P, {"neighbor_id_2d": nb, "Delta": 0.4, "voxel": voxel}, sp, ap, **kw)
+    t_host = time.perf_counter() - t0
+    times = []
+    for _ in range(reps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        inst = geometry_gpu.compile_instance(voxel, 0.4, par, D0, sp, ap, **kw)
+        torch.cuda.synchronize(dev)
+        times.append(time.perf_counter() - t0)
+    eng = BatchedEngine(_lib.PREC_F32)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    eng.add(inst)
+    torch.cuda.synchronize(dev)
+    t_add_dev = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    eng.add(host)
+    t_add_host = time.perf_counter() - t0
+    eng.close()
+    return {"voxels": int(n), "workload": "scarred fibre shell, MS, anisotropic D0 (edge terms)",
+            "host_numpy_s": t_host, "device_s": min(times), "device_s_all": times,
+            "speedup": t_host / min(times), "engine_add_device_tables_s": t_add_dev,
+            "engine_add_host_tables_s": t_add_host}
+
+
 def aniso_leg(args, dev, tune=None, count=16):
     """Anisotropic tensors (rule-based fibre field, every cross term present):
     ``count`` seeded shells of n_min..n_max voxels through the edge-term kernel,
@@ -488,10 +539,11 @@ def serving_leg(args, plain_rate, dev):
     reqs = serving.poisson_requests(args.serving_requests, seed=args.seed)
     free = torch.cuda.mem_get_info(dev)[0]
     srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
-                         stream=torch.cuda.current_stream(dev).cuda_stream)
+                         stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True)
     done, totals = srv.run(reqs)
     srv.close()
     out = serving.summarize(done, totals, reqs)
+    out["builder"] = "device (neighbour table, P_2d and operator tables on the GPU, one stream per builder thread)"
     # FIFO single-server schedule of the same requests at the plain FP64 rate
     t = 0.0
     lat = []
@@ -632,6 +684,12 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"electrogram": egm_leg(args, dev)}), flush=True)
+        return 0
+    if args.geometry_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"geometry": geometry_leg(args, dev)}), flush=True)
         return 0
     if args.aniso_only:
         import torch

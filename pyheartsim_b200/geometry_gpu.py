@@ -152,6 +152,11 @@ class DeviceInstance(CompiledInstance):
         self._desc = d
         return d
 
+    def release_tables(self):
+        """Drop the device tables (after the engine has copied them)."""
+        for k in ("nb6_t", "coef6_t", "cw_t", "mask6_t", "vflags_t", "vparams_t", "nb_edge_t", "coef_edge_t"):
+            setattr(self, k, None)
+
     def host_tables(self):
         """The tables as numpy arrays (the names :class:`CompiledInstance` uses)."""
         g = lambda t: None if t is None else t.cpu().numpy()

@@ -19,6 +19,7 @@ engine's reductions do not depend on team size or batch-mates, every result is
 bit-identical to running the same request alone.
 """
 import math
+import threading
 import time
 from collections import deque
 from concurrent.futures import ThreadPoolExecutor
@@ -57,9 +58,22 @@ def poisson_requests(count, rate_per_s=20.0, n_min=20_000, n_max=1_000_000, dur_
     return [Request(i, float(t[i]), n[i], d[i], m[i], seed * 100_003 + i) for i in range(count)]
 
 
-def build(req, tol=1e-7, restart=20):
-    """Compile a request into an FP32 early-exit instance (shell geometry with scar)."""
+_tls = threading.local()
+
+
+def build(req, tol=1e-7, restart=20, device=False):
+    """Compile a request into an FP32 early-exit instance (shell geometry with
+    scar).  ``device``: neighbour table, P_2d and operator tables on the GPU,
+    on a stream of the calling builder thread (same instance as the host path)."""
     i = 2 * (req.seed % 1000) + req.model        # parity of i selects the model in shell_case
+    if device:
+        import torch
+        if getattr(_tls, "stream", None) is None:
+            _tls.stream = torch.cuda.Stream()
+        with torch.cuda.stream(_tls.stream):
+            inst, _ = workloads.shell_case_device(i, req.n_target, req.seed // 1000, t_phys=req.duration_ms, tol=tol,
+                                                  restart=restart, stream=_tls.stream)
+        return inst
     inst, _, meta = workloads.shell_case(i, req.n_target, req.seed // 1000, t_phys=req.duration_ms, tol=tol,
                                          restart=restart)
     return inst
@@ -92,12 +106,12 @@ class _Inline:
 
 class Server:
     def __init__(self, hbm_budget_bytes, steps_per_launch=50, rebalance_every=8, build_threads=8, tol=1e-7,
-                 stream=None, engine=None, builder=None, footprint=None):
+                 stream=None, engine=None, builder=None, footprint=None, device_build=False):
         self.budget = int(hbm_budget_bytes)
         self.S = int(steps_per_launch)
         self.rebalance_every = int(rebalance_every)
         self.tol = tol
-        self.builder = builder or (lambda r: build(r, self.tol))
+        self.builder = builder or (lambda r: build(r, self.tol, device=device_build))
         self.footprint = footprint or footprint_bytes
         self.engine = engine if engine is not None else BatchedEngine(_lib.PREC_F32)
         self.engine.set_profile(True)
@@ -135,6 +149,8 @@ class Server:
                 queue.popleft()
                 r.inst = inst
                 r.slot = self.engine.add(inst)
+                if hasattr(inst, "release_tables"):
+                    inst.release_tables()          # the engine holds its own copy
                 r.admit_s = time.perf_counter() - t0
                 r.fp = fp
                 self.used += fp

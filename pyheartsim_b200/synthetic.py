@@ -78,8 +78,9 @@ def shell_for_size(n_target, seed=0, Delta=0.4, wall=3, base=(25.0, 20.0, 18.0),
 
 
 def scar(ijk, nb, coverage, rng, c_border=0.1, n_blobs=6, width=8.0):
-    """(c_scale, node_flag): Gaussian-blob field thresholded to ``coverage``;
-    c = 0 inside, ``c_border`` on the one-voxel ring around the scar, 1 elsewhere."""
+    """Conductivity scale (n,): Gaussian-blob field thresholded to ``coverage``;
+    0 inside, ``c_border`` on the one-voxel ring around the scar (face
+    neighbours ``nb[:, :6]``), 1 elsewhere."""
     n = ijk.shape[0]
     c = np.ones(n)
     if coverage <= 0:
@@ -143,8 +144,20 @@ def make_case(ijk, Delta, model, dt_phys, t_phys, s1_ids, *, c_phys=None, s2_ids
     divided by 6, c multiplied by 6).  ``D0``: (n, 3, 3) diffusion tensors
     (default identity, the reference's load_fiber)."""
     n = ijk.shape[0]
-    ts = 1 if model == 0 else 6
     nb = lattice_neighbors(ijk)
+    sp, ap, par = case_parameters(n, model, dt_phys, t_phys, s1_ids, c_phys=c_phys, s2_ids=s2_ids, flag=flag,
+                                  s1_t=s1_t, s1_s2=s1_s2, start=start, cycle=cycle, node_flag=node_flag,
+                                  c_scale=c_scale)
+    P = heart_model_equation_parts(sp, n, D0, nb, par)
+    geom = {'neighbor_id_2d': nb, 'Delta': Delta, 'voxel': ijk * Delta}
+    return n, P, geom, sp, ap
+
+
+def case_parameters(n, model, dt_phys, t_phys, s1_ids, *, c_phys=None, s2_ids=None, flag=4, s1_t=0.0, s1_s2=0.0,
+                    start=10.0, cycle=300.0, node_flag=None, c_scale=None):
+    """(simulation_parameters, arrhythmia_parameters, parameter) of make_case,
+    without the geometry tables (for builders that make those on the device)."""
+    ts = 1 if model == 0 else 6
     if c_phys is None:
         c_phys = 1.0 if model == 0 else 1.6
     c = np.full(n, c_phys * ts)
@@ -158,9 +171,7 @@ def make_case(ijk, Delta, model, dt_phys, t_phys, s1_ids, *, c_phys=None, s2_ids
           's1_t': s1_t / ts, 's1_s2_delta_t': s1_s2 / ts,
           'node_flag': np.zeros(n, dtype=np.int64) if node_flag is None else node_flag}
     par = model_parameters(model, n, c)
-    P = heart_model_equation_parts(sp, n, D0, nb, par)
-    geom = {'neighbor_id_2d': nb, 'Delta': Delta, 'voxel': ijk * Delta}
-    return n, P, geom, sp, ap
+    return sp, ap, par
 
 
 def electrodes_grid(nx, ny, Delta, nside=4, z=1.0):

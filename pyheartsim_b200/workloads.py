@@ -53,6 +53,33 @@ def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-
                                         "pacing_ms": pacing_ms, "fibres": bool(fibres)}
 
 
+def shell_case_device(i, n_target, seed, t_phys=500.0, scar_max=0.3, tol=1e-5, restart=20, save_h=False,
+                      pacing_ms=2.0, fibres=False, stream=None):
+    """The instance of :func:`shell_case` (same geometry, scar, pacing site and
+    tables), built on the GPU: the neighbour table, P_2d and the operator
+    tables come from the device geometry path; only the face neighbours the
+    scar generator needs come back to the host."""
+    from . import geometry_gpu
+    rng = np.random.default_rng(seed * 1000 + i)
+    ijk = _shell_scaled(n_target, seed * 1000 + i)
+    nb18, _ = geometry_gpu.lattice_neighbors(ijk, order=False, stream=stream)
+    nb6 = nb18[:, :6].cpu().numpy()
+    cov = float(rng.uniform(0.0, scar_max))
+    c_scale = synthetic.scar(ijk, nb6, cov, rng)
+    healthy = np.where(c_scale == 1.0)[0]
+    centre = ijk[healthy[int(rng.integers(0, healthy.size))]]
+    s1 = np.where(np.sum((ijk - centre) ** 2, axis=1) <= 9)[0]
+    model = i % 2
+    dt_phys = 0.05 if model == 0 else 0.02
+    n = ijk.shape[0]
+    sp, ap, par = synthetic.case_parameters(n, model, dt_phys, t_phys, s1, flag=4, c_scale=c_scale)
+    D0 = synthetic.fibre_tensors(ijk) if fibres else None
+    inst = geometry_gpu.compile_instance(ijk * 0.4, 0.4, par, D0, sp, ap, full_cycles=False, tol=tol, atol=1e-5,
+                                         restart=restart, pacing_duration=pacing_ms / sp['time_scale'],
+                                         save_h=save_h, stream=stream)
+    return inst, {"index": i, "n": n, "model": model, "scar": cov, "pacing_ms": pacing_ms, "fibres": bool(fibres)}
+
+
 def _build_one(args):
     i, n_target, seed, kw = args
     inst, _, meta = shell_case(i, n_target, seed, **kw)

@@ -126,3 +126,21 @@ def test_row_order_matches_host_locality_order(cuda_device):
     host = instance.locality_order({"voxel": ijk * 0.4, "Delta": 0.4}, ijk.shape[0], "rows")
     np.testing.assert_array_equal(order.cpu().numpy(), host)
     np.testing.assert_array_equal(nb18.cpu().numpy(), geometry.lattice_neighbors(ijk))
+
+
+def test_device_built_workload_instance_equals_host_built(cuda_device):
+    """The serving / benchmark shell builder on the device gives the host
+    builder's instance (same geometry, scar, pacing and tables)."""
+    from pyheartsim_b200 import workloads
+    host, _, _ = workloads.shell_case(3, 30_000, 2, t_phys=50.0, tol=1e-7)
+    dev, meta = workloads.shell_case_device(3, 30_000, 2, t_phys=50.0, tol=1e-7)
+    t = dev.host_tables()
+    np.testing.assert_array_equal(dev.order, host.order)
+    np.testing.assert_array_equal(t["nb6"], host.nb6)
+    np.testing.assert_array_equal(t["coef6"], host.coef6)
+    np.testing.assert_array_equal(t["vflags"], host.vflags)
+    assert (dev.cw is None) == (host.cw is None)
+    if host.cw is not None:
+        np.testing.assert_array_equal(t["cw"], host.cw)
+    np.testing.assert_array_equal(dev.stim, host.stim)
+    assert dev.n_steps == host.n_steps and dev.model == host.model

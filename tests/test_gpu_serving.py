@@ -26,7 +26,8 @@ def test_result_alone_equals_result_in_the_mix(cuda_device):
     mix = _small_requests()
     mix[1].arrival_s = 0.05
     mix[2].arrival_s = 0.10
-    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40, rebalance_every=2)
+    # built on the device this time: the same instances, so the same results
+    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40, rebalance_every=2, device_build=True)
     done, totals = srv.run(mix, keep_history=True)
     srv.close()
     assert len(done) == 3
