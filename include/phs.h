@@ -296,6 +296,19 @@ typedef struct phs_operator_tables_args {
 } phs_operator_tables_args;
 int phs_operator_tables(phs_operator_tables_args* args);
 
+/* ------------------------------------------------ electrogram analysis (device)
+ * Electrode activation times, utility/lat_map.py:20-27: lat_out[e] (int32) =
+ * first t maximising -(egm[t+1][e] - egm[t][e]) (NaN counts as the largest),
+ * minus the minimum over electrodes.  egm [T][n_e], f64 (is_f64) or f32.      */
+int phs_electrode_lat(int64_t T, int64_t n_e, const void* egm, int is_f64, int32_t* lat_out, void* stream);
+/* Conduction velocity, utility/conduction_velocity.py:23-70: for each of n_e
+ * points xyz [n_e][3] with activation times lat [n_e] (f64), the minimum-norm
+ * least-squares plane through the points within `radius` (itself included;
+ * the reference uses 8 mm); v_vec [n_e][3] = grad / |grad|^2, v_mag [n_e] =
+ * 1 / |grad|, NaN with fewer than 4 points or |grad|^2 <= 1e-8.             */
+int phs_conduction_velocity(int64_t n_e, const double* xyz, const double* lat, double radius, double* v_vec,
+                            double* v_mag, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -183,6 +183,10 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "phs_operator_flags": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, c_int32_p, ctypes.c_void_p]),
     "phs_operator_tables": (ctypes.c_int, [ctypes.POINTER(OperatorTablesArgs)]),
+    "phs_electrode_lat": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_conduction_velocity": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _lib = None
