@@ -42,3 +42,37 @@ def test_cv_random_points_match_oracle(cuda_device):
     np.testing.assert_array_equal(np.isnan(m), np.isnan(mo))
     np.testing.assert_allclose(v, vo, rtol=CV_RTOL, atol=0)
     np.testing.assert_allclose(m, mo, rtol=CV_RTOL, atol=0)
+
+
+def test_result_file_from_the_device_history(tmp_path, cuda_device):
+    """Run an instance, compute its electrogram and electrode LAT on the device,
+    stream the reference's result file from the device history, read it back."""
+    from pyheartsim_b200 import instance, results
+    from pyheartsim_b200.engine import BatchedEngine
+    from pyheartsim_b200.simulation import unipolar_electrogram_gpu
+    from tests import gpu_cases
+    (n, P, geom, sp, ap), pdur = gpu_cases.small_shell_ms(t_phys=30.0)
+    inst = instance.compile_instance(n, P, geom, dict(sp), dict(ap), full_cycles=False, tol=1e-7, restart=20,
+                                     pacing_duration=pdur)
+    eng = BatchedEngine()
+    s = eng.add(inst)
+    while not eng.finished(s):
+        eng.advance(100)
+    u, h = eng.history(s, with_h=True)
+    ids = np.arange(0, n, 97)
+    egm = unipolar_electrogram_gpu.compute(geom["voxel"][ids] + 1.5, geom["voxel"], None, P[:, 20], u.astype(np.float64),
+                                           geom["Delta"], geom["neighbor_id_2d"])
+    lat = analysis.compute_electrode_lat(egm)
+    t = inst.sample_times(u.shape[0])
+    path = results.save_simulation_results(tmp_path / "shell_simulation_results", eng, s, geometry_flag=1,
+                                           electrogram=egm, save_all=True, physical_time=t, lat_electrode=lat,
+                                           chunk=7)
+    eng.close()
+    f = np.load(path)
+    assert f.files == ["geometry_flag", "electrogram_unipolar", "action_potential", "h", "physical_time",
+                       "lat_electrode"]
+    np.testing.assert_array_equal(f["action_potential"], u)
+    np.testing.assert_array_equal(f["h"], h)
+    np.testing.assert_array_equal(f["electrogram_unipolar"], egm)
+    np.testing.assert_array_equal(f["lat_electrode"], lat)
+    np.testing.assert_array_equal(f["physical_time"], t)
