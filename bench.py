@@ -36,6 +36,7 @@ METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99
 # multiplied by the voxels and steps of one launch below.
 STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 232.4
 STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.05
+BALANCE_LAUNCHES = 10   # launches per team-balancing round in the pre-steps
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
 
 
@@ -198,19 +199,23 @@ def run_b200(args):
         from pyheartsim_b200 import autotune
         tune = autotune.tune(eng, steps=S, stream=stream)
         pre = max(0, pre - S * 2 * len(tune.get("table", [])))
-    for _ in range(pre // S):
+    # team sizes from each instance's measured cost: the last BALANCE_LAUNCHES x
+    # 3 launches of the (untimed) pre-steps run with the phase timers on, in
+    # three rounds that each re-split the CTAs by the cost measured in the
+    # round before (windows of 100 steps: the Arnoldi counts of single steps
+    # vary a lot); then W warm-up steps on the final plan (graph capture)
+    rounds = 3
+    bal = min(BALANCE_LAUNCHES, max(1, (pre // S) // (rounds + 1)))
+    for _ in range(pre // S - rounds * bal):
         eng.advance(S, stream=stream, sync=False)
-    # team sizes from each instance's cost over the warm-up window: the first
-    # rebalance starts the window, the second applies it; the last warm-up
-    # launches capture the CUDA graph of the new plan
     eng.set_profile(True)
-    for _ in range(3):
+    for _ in range(rounds):
         eng.rebalance()
-        for _ in range(max(1, (W // 4) // S)):
+        for _ in range(bal):
             eng.advance(S, stream=stream, sync=False)
     eng.rebalance()
     eng.set_profile(False)
-    for _ in range(max(1, (W // 4) // S)):
+    for _ in range(max(1, W // S)):
         eng.advance(S, stream=stream, sync=False)
     torch.cuda.synchronize(dev)
     info0 = [eng.info(s) for s in slots]
@@ -339,6 +344,11 @@ def phase_profile(eng, slots, S, stream):
     out = {k: round(v / len(slots), 5) for k, v in acc.items()}
     out["team_ms_per_step_min"] = round(min(totals), 5)
     out["team_ms_per_step_max"] = round(max(totals), 5)
+    # CTA-weighted busy fraction of the launch: teams that finish their steps
+    # early leave their CTAs idle until the slowest team is done
+    teams = np.array([r[2] for r in per], dtype=np.float64)
+    busy = np.array(totals)
+    out["cta_utilization"] = round(float((teams * busy).sum() / (teams.sum() * busy.max())), 4)
     out["per_instance"] = sorted(per, key=lambda r: -r[4])[:12]
     return out
 

@@ -681,6 +681,15 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     // ---- sample / activation bookkeeping of the state in u (after step s-1)
+    // the same with the activation entry already loaded (lat_n; read only when
+    // un >= 0.5 after a completed step)
+    auto sample_loaded = [&](long long n, T un, T hn, int32_t lat_n, long long done_step) {
+        if (pending >= 0) {
+            I.hist_u[(size_t)pending * N + n] = un;
+            if (I.save_h) I.hist_h[(size_t)pending * N + n] = hn;
+        }
+        if (done_step >= 0 && un >= T(0.5) && lat_n < 0) I.lat[n] = (int32_t)done_step;
+    };
     auto sample_voxel = [&](long long n, T un, T hn, long long done_step) {
         if (pending >= 0) {
             I.hist_u[(size_t)pending * N + n] = un;
@@ -735,18 +744,39 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 else if (t == 2) pf_slice(I.vflags, 1, tile + P);
                 else pf_slice(I.vparams, 5 * sizeof(T), tile + P);
             }
+            // every load of the tile before its first store: plain loads cannot
+            // move across stores the compiler must assume may alias them
+            T un[VPT], hn[VPT];
+            uint8_t fl[VPT];
+            int32_t lt[VPT];
+#pragma unroll
+            for (int v = 0; v < VPT; ++v) {
+                const long long n = voxel(tile, v);
+                un[v] = T(0);
+                hn[v] = T(0);
+                fl[v] = 0;
+                lt[v] = 0;
+                if (n < N) {
+                    un[v] = I.u[n];
+                    hn[v] = hin[n];
+                    fl[v] = __ldg(I.vflags + n);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < VPT; ++v) {
+                const long long n = voxel(tile, v);
+                if (n < N && step > 0 && un[v] >= T(0.5)) lt[v] = I.lat[n];
+            }
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
                 if (n < N) {
-                    const T un = I.u[n], hn = hin[n];
-                    const uint8_t f = __ldg(I.vflags + n);
-                    sample_voxel(n, un, hn, step - 1);
+                    sample_loaded(n, un[v], hn[v], lt[v], step - 1);
                     T p[5];
                     params_of(n, p);
-                    const T J = (f & stim_bits & 3u) ? I.jmag : T(0);
+                    const T J = (fl[v] & stim_bits & 3u) ? I.jmag : T(0);
                     T us, hs;
-                    rk4(I.model, un, hn, J, p, I.dt, us, hs);
+                    rk4(I.model, un[v], hn[v], J, p, I.dt, us, hs);
                     hout[n] = hs;
                     Us[n] = us;
                 }
@@ -992,10 +1022,16 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             const T* src = (act == ACT_ZERO_B) ? I.b : I.x;
             for (int tile = rank; tile < I.n_tiles; tile += P) {
                 if (threadIdx.x == 0) pf_slice(src, sizeof(T), tile + P);
+                T cv[VPT];
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
                     const long long n = voxel(tile, v);
-                    if (n < N) I.u[n] = src[n];
+                    cv[v] = (n < N) ? src[n] : T(0);
+                }
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    const long long n = voxel(tile, v);
+                    if (n < N) I.u[n] = cv[v];
                 }
             }
         } else {  // ACT_FAIL
