@@ -154,10 +154,11 @@ int64_t phs_engine_launch_count(phs_engine* eng);
                                           that is never launched; its bounded barrier gives up after
                                           4 s and advance() returns PHS_ERR_TIMEOUT (the engine is
                                           then unusable, the CUDA context is not affected)        */
-#define PHS_CFG_AUTO_BALANCE 5   /* 1 (default): the second and third advance() after an instance
-                                    is added or removed first call phs_engine_rebalance, so team
-                                    sizes follow the Arnoldi iterations measured since; 0: team
-                                    sizes change only on explicit rebalance                  */
+#define PHS_CFG_AUTO_BALANCE 5   /* 1 (default): after an instance is added or removed, the next
+                                    launch runs with the phase timers on (if they are off) and
+                                    the two after it first call phs_engine_rebalance, so team
+                                    sizes follow the measured cost; then the timers go off
+                                    again.  0: team sizes change only on explicit rebalance  */
 int phs_engine_config(phs_engine* eng, int key, int64_t value);
 /* Compiled step-kernel variants of a precision: count, and per variant the
  * minimum CTAs per SM it was compiled for and its register count (arrays of at

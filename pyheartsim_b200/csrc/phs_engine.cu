@@ -1198,6 +1198,7 @@ struct phs_engine {
     bool auto_balance = true;  // rebalance on the 2nd and 3rd advance after the instance set changes
     int auto_left = 0;
     long long auto_mark = 0;   // launch count when the set changed / at the last automatic rebalance
+    bool auto_prof = false;    // the phase timers were switched on by the automatic balancing
     // CUDA graphs of the launch sequence, keyed by steps per launch
     std::map<long long, cudaGraphExec_t> graphs;
     bool graphs_ok = true;
@@ -1616,11 +1617,24 @@ template <typename T>
 int advance_impl(phs_engine* e, long long n_steps, int ctas_per_sm, cudaStream_t stream, bool sync) {
     if (e->broken) return PHS_ERR_STATE;
     if (n_steps <= 0) return PHS_OK;
+    // automatic balancing: the launch after an instance set change runs with the
+    // phase timers on (unless the caller has them on already), the next two
+    // re-split the CTAs by the measured cost, then the timers go off again
+    if (e->auto_balance && e->auto_left > 0 && !e->profile) {
+        const int rp = phs_engine_config(e, PHS_CFG_PROFILE, 1);
+        if (rp != PHS_OK) return rp;
+        e->auto_prof = true;
+    }
     if (e->auto_balance && e->auto_left > 0 && e->launches > e->auto_mark) {
         const int rb = phs_engine_rebalance(e);
         if (rb != PHS_OK) return rb;
         e->auto_left -= 1;
         e->auto_mark = e->launches;
+        if (e->auto_left == 0 && e->auto_prof) {
+            const int rp = phs_engine_config(e, PHS_CFG_PROFILE, 0);
+            if (rp != PHS_OK) return rp;
+            e->auto_prof = false;
+        }
     }
     // the edge-term kernel only when an unfinished instance is anisotropic
     bool edge = false;
