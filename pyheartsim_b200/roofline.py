@@ -6,8 +6,9 @@ one value + a presence byte; 6 s otherwise).  Neighbour values read by the
 stencil are assumed to hit in cache (their owners stream them in the same
 phase).
 
-  RHS        read u, h, flags, nb[6] (int32), coefficients; write x, h', b, V0
-             = 6 s + 25 + cb
+  RHS pass 1 read u, h, flags; write h', u* (basis column 1)     = 4 s + 1
+  RHS pass 2 read u*, flags, nb[6] (int32), coefficients; write x, b, V0
+                                                                 = 4 s + 25 + cb
   phase A_j  read V_j, nb, coefficients, V_0..V_{j-1}; write w  = (j + 2) s + 24 + cb
   phase C_j  read w, V_0..V_j; write V_{j+1}                     = (j + 3) s
   update     read x, V_0..V_{k-1}; write u                       = (k + 2) s
@@ -16,13 +17,12 @@ phase).
 
 A solve with k Arnoldi steps therefore costs
   B(k) = RHS + (k + 2) s + k (5 s + 24 + cb) + s k (k - 1),
-e.g. 81 + 68 k + 4 k^2 bytes in FP32 with six stored coefficients, and
-62 + 49 k + 4 k^2 with isotropic rows.
+e.g. 90 + 68 k + 4 k^2 bytes in FP32 with six stored coefficients, and
+71 + 49 k + 4 k^2 with isotropic rows.
 
 Anisotropic rows (edge cross terms) add the edge table, 12 int32 indices and
-six coefficients = 48 + 6 s, to every operator application (the RHS and each
-A_j), and their RHS phase passes u* through memory (write + read, 2 s) and
-reads the flags twice (+1): in FP32 +97 bytes per step and +72 per Arnoldi step.
+six coefficients = 48 + 6 s, to every operator application (the RHS stencil
+and each A_j): in FP32 +72 bytes per step and +72 per Arnoldi step.
 """
 
 
@@ -31,7 +31,7 @@ def coef_bytes(s, iso):
 
 
 def bytes_rhs(s, cb):
-    return 6 * s + 25 + cb
+    return 8 * s + 26 + cb
 
 
 def edge_bytes(s):
@@ -49,7 +49,7 @@ def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, 
     if guess:     # read the increment in the RHS phase; read and rewrite it in the final update
         per_voxel += steps * s + 2 * s * (solves or 0)
     if edge:
-        per_voxel += steps * (edge_bytes(s) + 2 * s + 1) + edge_bytes(s) * k_sum
+        per_voxel += steps * edge_bytes(s) + edge_bytes(s) * k_sum
     return voxels * per_voxel
 
 

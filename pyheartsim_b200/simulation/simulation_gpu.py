@@ -4,9 +4,9 @@
 arrhythmia_parameters)`` has the reference's signature and returns the same
 arrays ``(u_hist (S, n), h_hist (S, n), physical_time (S,))``
 (simulation/simulation_gpu.py:261-409).  The whole run executes on the GPU
-through ``phs_simulate`` (include/phs.h): fused RK4 + CN right-hand side and
-restarted GMRES in one persistent sm_100a kernel, the stimulus schedule and
-the 1 kHz history on the device.
+through ``phs_simulate`` (include/phs.h): RK4 reaction, the CN right-hand
+side and restarted GMRES in one persistent sm_100a kernel, the stimulus
+schedule and the 1 kHz history on the device.
 
 Differences from the reference, all deliberate:
 * the plain form computes in FP64 (the reference stores FP32); pass
