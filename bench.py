@@ -299,6 +299,10 @@ def run_b200(args):
             line["geometry"] = geometry_leg(args, dev)
             del batch, insts
             line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
+            # latency below saturation: Poisson arrivals offering half the batched
+            # throughput, shorter requests (100-400 ms)
+            line["serving_half_load"] = serving_leg(args, line["plain_fp64"]["value"], dev, load=(0.5, value),
+                                                    dur_ms=(100.0, 400.0), count=12)
             line["electrogram"] = egm_leg(args, dev)
             line["cpu_baseline"] = cpu_leg(args)
     if world > 1:
@@ -539,14 +543,26 @@ def accuracy_leg(dev, tol):
             "max_abs_dvm": float(np.abs(u64 - u32).max()), "voxels": int(n), "ms": 60.0, "tol": tol}
 
 
-def serving_leg(args, plain_rate, dev):
-    """Continuous batching under Poisson arrivals (20/s, 20k-1M voxels, 200-2000 ms,
-    random model and pacing site): latency percentiles and served throughput.
-    The plain-FP64-serial comparison is an estimate from the measured plain rate
-    (running it for real would take hours)."""
+def serving_leg(args, plain_rate, dev, load=None, dur_ms=(200.0, 2000.0), count=None):
+    """Continuous batching under Poisson arrivals (20k-1M voxels, random model
+    and pacing site): latency percentiles and served throughput.  Default: 20
+    requests/s of 200-2000 ms, about 10x what one B200 can serve (the overload
+    case).  ``load = (fraction, capacity)``: instead, the arrival rate whose
+    requests offer that fraction of ``capacity`` voxel-steps/s (the measured
+    batched throughput).  The plain-FP64-serial comparison is an estimate from
+    the measured plain rate ``plain_rate`` (running it for real would take
+    hours)."""
     import torch
     from pyheartsim_b200 import serving
-    reqs = serving.poisson_requests(args.serving_requests, seed=args.seed)
+    count = count or args.serving_requests
+    rate = 20.0
+    if load is not None:
+        frac, capacity = load
+        probe = serving.poisson_requests(count, rate_per_s=1.0, dur_ms=dur_ms, seed=args.seed)
+        # voxel-steps of a request: physical dt 0.05 ms (MS) or 0.02 ms (AP)
+        work = np.mean([r.n_target * r.duration_ms / (0.05 if r.model == 0 else 0.02) for r in probe])
+        rate = frac * capacity / work
+    reqs = serving.poisson_requests(count, rate_per_s=rate, dur_ms=dur_ms, seed=args.seed)
     free = torch.cuda.mem_get_info(dev)[0]
     srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
                          stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True)
@@ -562,6 +578,8 @@ def serving_leg(args, plain_rate, dev):
         lat.append(t - r.arrival_s)
     out["plain_fp64_serial_estimate"] = {"p50_latency_s": float(np.percentile(lat, 50)),
                                          "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": t}
+    out["arrival_rate_per_s"] = rate
+    out["durations_ms"] = list(dur_ms)
     return out
 
 
