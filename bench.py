@@ -56,6 +56,9 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-7)
     p.add_argument("--t-phys", type=float, default=500.0, help="simulated ms per instance")
     p.add_argument("--no-extras", action="store_true", help="skip e2e, plain-FP64, accuracy and CPU legs")
+    p.add_argument("--no-accuracy", action="store_true", help="skip the accuracy leg (c1, c2, c3 sample)")
+    p.add_argument("--c2-walls", type=int, nargs="*", default=[3, 8], help="wall thicknesses of the c2 runs")
+    p.add_argument("--accuracy-only", action="store_true", help="run only the accuracy leg")
     p.add_argument("--no-tune", action="store_true", help="use the default step-kernel variant")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--serving-requests", type=int, default=16)
@@ -178,14 +181,15 @@ def run_b200(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
-    from pyheartsim_b200 import _lib, roofline, workloads
+    from pyheartsim_b200 import _lib, geometry_gpu, roofline, workloads
     from pyheartsim_b200.engine import BatchedEngine
 
     seed = args.seed + 7919 * rank
-    batch = workloads.batched_shells(args.instances, args.n_min, args.n_max, seed, tol=args.tol,
-                                     t_phys=args.t_phys)
-    insts = [b[0] for b in batch]
-    ns = np.array([m["n"] for _, m in batch], dtype=np.int64)
+    # reference-style inputs (P_2d, neighbour table, parameter dicts) built on
+    # host processes, compiled into engine instances on the device
+    cases = workloads.batched_inputs(args.instances, args.n_min, args.n_max, seed, t_phys=args.t_phys)
+    insts = [compile_case(c, m, args.tol) for c, m in cases]
+    ns = np.array([m["n"] for _, m in cases], dtype=np.int64)
     S = max(1, args.steps_per_launch)
     K = (args.steps + S - 1) // S * S
     W = max(3, (args.warmup + S - 1) // S * S)
@@ -193,6 +197,8 @@ def run_b200(args):
 
     eng = BatchedEngine(_lib.PREC_F32)
     slots = [eng.add(x) for x in insts]
+    for x in insts:
+        x.release_tables()
     pre = (args.pre_steps // S) * S
     tune = None
     if not args.no_tune:
@@ -291,13 +297,16 @@ def run_b200(args):
             "phases_ms_per_step": phases}
 
     if not args.no_extras:
-        line["e2e"] = e2e_leg(args, insts, ns, pre + K, dev)
+        del insts
+        line["e2e"] = e2e_leg(args, cases, dev)
         if rank == 0 and world == 1:
-            line["plain_fp64"] = plain_leg(args, batch, value, dev)
-            line["accuracy"] = accuracy_leg(dev, args.tol)
+            line["e2e_dropin_c1"] = dropin_c1_leg(dev)
+            line["plain_fp64"] = plain_leg(args, cases, value, dev)
+            if not args.no_accuracy:
+                line["accuracy"] = accuracy_leg(dev, args.tol, walls=tuple(args.c2_walls))
             line["anisotropic"] = aniso_leg(args, dev, tune, count=args.aniso_instances)
             line["geometry"] = geometry_leg(args, dev)
-            del batch, insts
+            del cases
             line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
             # latency below saturation: Poisson arrivals offering half the batched
             # throughput, shorter requests (100-400 ms)
@@ -357,46 +366,98 @@ def phase_profile(eng, slots, S, stream):
     return out
 
 
-def e2e_leg(args, insts, ns, steps, dev):
-    """The drop-in path with host buffers: upload every instance, run ``steps``
-    steps, download the 1 kHz Vm history and the final state."""
+def compile_case(case, meta, tol, stream=None):
+    """Engine instance of one reference-style input set, compiled on the device
+    (FP32 early exit at ``tol``, restart 20, 1 kHz Vm history)."""
+    from pyheartsim_b200 import geometry_gpu
+    return geometry_gpu.compile_reference_inputs(*case, full_cycles=False, tol=tol, atol=1e-5, restart=20,
+                                                 save_h=False, pacing_duration=meta["pacing_ms"] / case[3]["time_scale"],
+                                                 stream=stream)
+
+
+def e2e_leg(args, cases, dev):
+    """The whole batched job through the public API, from the reference-style
+    inputs on the host (P_2d, neighbour table, voxel coordinates and parameter
+    dicts of every instance) to every instance's full 1 kHz Vm history and
+    final state on the host: upload and device compilation of the tables,
+    every instance run to its last step (500 ms: 10,000 steps for
+    Mitchell-Schaeffer, 25,000 for Aliev-Panfilov) with graph-replayed launches
+    on a CUDA stream, download.  Wall time of each part."""
     import torch
     from pyheartsim_b200 import _lib
     from pyheartsim_b200.engine import BatchedEngine
+    stream = torch.cuda.Stream(dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        insts = [compile_case(c, m, args.tol, stream=stream) for c, m in cases]
     eng = BatchedEngine(_lib.PREC_F32)
     slots = [eng.add(x) for x in insts]
-    h2d = sum(x.nb6.nbytes + (x.cw.nbytes + x.mask6.nbytes if x.cw is not None else x.coef6.nbytes)
-              + x.vflags.nbytes + x.stim.nbytes + (x.vparams.nbytes if x.vparams is not None else 0)
-              for x in insts)
-    S = max(1, args.steps_per_launch)
-    done = 0
-    while done < steps:
-        k = min(S * 10, steps - done)
-        eng.advance(k, sync=True)
-        done += k
+    for x in insts:
+        x.release_tables()
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    h2d = sum(c[1].nbytes + np.asarray(c[2]['neighbor_id_2d']).size * 4 + np.asarray(c[2]['voxel']).nbytes
+              for c, _ in cases)
+    S = 10 * max(1, args.steps_per_launch)
+    steps_total = max(x.n_steps for x in insts)
+    k = 0
+    while not all(eng.finished(s) for s in slots):
+        for _ in range(10):
+            eng.advance(S, stream=stream, sync=False)
+        eng.advance(S, stream=stream, sync=True)     # refresh the finished flags: finished instances leave the plan
+        k += 11
+    t2 = time.perf_counter()
     d2h = 0
     for s in slots:
         hist = eng.history(s)
         u, h, lat = eng.state(s)
         d2h += hist.nbytes + u.nbytes + h.nbytes + lat.nbytes
-    t1 = time.perf_counter()
+    t3 = time.perf_counter()
+    vs = float(sum(x.n_voxel * x.n_steps for x in insts))
     eng.close()
-    v = float(ns.sum()) * steps / (t1 - t0)
-    return {"value": v, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
-            "steps": int(steps), "seconds": t1 - t0}
+    return {"value": vs / (t3 - t0), "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d / steps_total,
+            "d2h_bytes_per_step": d2h / steps_total, "voxel_steps": vs, "steps_longest_instance": int(steps_total),
+            "seconds": t3 - t0, "compile_upload_s": t1 - t0, "run_s": t2 - t1, "download_s": t3 - t2,
+            "launches": int(k), "run_only_value": vs / (t2 - t1),
+            "path": "reference-style inputs on the host -> device compile (geometry_gpu.compile_reference_inputs) "
+                    "-> engine, graph replay on a stream -> full 1 kHz history and final state on the host"}
 
 
-def plain_leg(args, batch, fast_value, dev):
+def dropin_c1_leg(dev):
+    """The drop-in call itself (simulation_gpu.compute, then
+    unipolar_electrogram_gpu.compute) on the plain sheet: 200 x 200 voxels,
+    500 ms = 10,000 steps, 16 electrodes; host inputs in, host arrays out, wall
+    time per call.  Plain FP64 (the reference's GMRES(50) full cycles) and the
+    FP32 early-exit form."""
+    from pyheartsim_b200 import workloads
+    from pyheartsim_b200.simulation import simulation_gpu, unipolar_electrogram_gpu
+    (n, P, geom, sp, ap), pdur, el = workloads.sheet_c1()
+    out = {"voxels": int(n), "steps": 10000, "electrodes": int(el.shape[0])}
+    for name, kw in (("plain_fp64", {}), ("fast_fp32", dict(dtype=np.float32, fast=True, tol=1e-7))):
+        t0 = time.perf_counter()
+        u, h, t = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur, **kw)
+        t1 = time.perf_counter()
+        mode = "fp64" if name == "plain_fp64" else "bf16x3"
+        egm = unipolar_electrogram_gpu.compute(el, geom['voxel'], None, P[:, 20], u, geom['Delta'],
+                                               geom['neighbor_id_2d'], mode=mode)
+        t2 = time.perf_counter()
+        out[name] = {"simulate_s": t1 - t0, "voxel_steps_per_s": n * 10000 / (t1 - t0), "electrogram_s": t2 - t1,
+                     "electrogram_mode": mode, "history_shape": list(u.shape)}
+    return out
+
+
+def plain_leg(args, cases, fast_value, dev):
     """Plain FP64 drop-in semantics (full GMRES(50) cycles, FP64) on the median
-    instance, same simulated window as the timed batch."""
+    instance of the batch, one instance on the whole GPU: throughput, the byte
+    model's roofline (k = m = 50 Arnoldi steps per cycle, one true-residual test
+    per cycle) and the device phase times."""
     import torch
-    from pyheartsim_b200 import _lib, workloads
+    from pyheartsim_b200 import _lib, roofline, workloads
     from pyheartsim_b200.engine import BatchedEngine
-    ns = np.array([m["n"] for _, m in batch])
+    ns = np.array([m["n"] for _, m in cases])
     i = int(np.argsort(ns)[len(ns) // 2])
-    meta = batch[i][1]
+    meta = cases[i][1]
     sizes = workloads.batch_sizes(args.instances, args.n_min, args.n_max, args.seed)
     inst, _, _ = workloads.shell_case(i, int(sizes[i]), args.seed, fast=False)
     eng = BatchedEngine(_lib.PREC_F64)
@@ -405,6 +466,7 @@ def plain_leg(args, batch, fast_value, dev):
     pre = min(args.pre_steps, 400)
     eng.advance(pre, stream=stream, sync=True)
     steps = 20
+    info0 = eng.info(slot)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
@@ -413,10 +475,28 @@ def plain_leg(args, batch, fast_value, dev):
     torch.cuda.synchronize(dev)
     ms = ev0.elapsed_time(ev1)
     info = eng.info(slot)
+    k_sum = info["arnoldi_steps"] - info0["arnoldi_steps"]
+    k_sq = info["arnoldi_sq"] - info0["arnoldi_sq"]
+    cycles = k_sum / 50.0
+    alg = roofline.algorithmic_bytes(8, meta["n"], steps, k_sum, k_sq, iso=inst.cw is not None, checks=cycles)
+    # device phase times over 4 more steps
+    eng.set_profile(True)
+    eng.advance(4, stream=stream, sync=True)
+    prof = eng.profile(slot)
     eng.close()
+    st = max(prof.pop("steps"), 1)
+    prof.pop("team_ctas", None)
+    it = prof.pop("arnoldi_iters")
+    pk, pk_src = peaks()
+    achieved = alg / (ms / 1e3) / 1e9
     v = meta["n"] * steps / (ms / 1e3)
     return {"value": v, "unit": "voxel-steps/s", "instance": i, "voxels": int(meta["n"]), "steps": steps,
-            "arnoldi_per_solve": info["arnoldi_steps"] / max(info["solves"], 1),
+            "ms_per_step": ms / steps, "arnoldi_per_step": k_sum / steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+                         "bytes_per_voxel_step": alg / (meta["n"] * steps),
+                         "note": "the 51-column FP64 Krylov basis of this instance fits in L2"},
+            "phases_ms_per_step": {k: round(v_ / st, 4) for k, v_ in prof.items()},
             "speedup_batched_fp32": fast_value / v}
 
 
@@ -528,19 +608,53 @@ def aniso_leg(args, dev, tune=None, count=16):
             "fibres": "D0 = 0.3 I + 0.7 e e^T, helix +-60 deg through the wall"}
 
 
-def accuracy_leg(dev, tol):
-    """Fast FP32 engine vs the plain FP64 path on a small scarred shell over a
-    whole activation: LAT error in units of dt and max |dVm|."""
-    from pyheartsim_b200.simulation import simulation_gpu
-    from tests import gpu_cases
-    (n, P, geom, sp, ap), pdur = gpu_cases.small_shell_ms(t_phys=60.0)
-    u64, _, _, lat64 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur, return_lat=True)
-    u32, _, _, lat32 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur,
-                                              dtype=np.float32, fast=True, tol=tol, return_lat=True)
-    both = (lat64 >= 0) & (lat32 >= 0)
-    return {"lat_err_max_dt": int(np.abs(lat64[both].astype(np.int64) - lat32[both]).max()) if both.any() else None,
-            "activated_same": bool(np.array_equal(lat64 >= 0, lat32 >= 0)),
-            "max_abs_dvm": float(np.abs(u64 - u32).max()), "voxels": int(n), "ms": 60.0, "tol": tol}
+def accuracy_leg(dev, tol, walls=(3, 8), c3_count=4):
+    """The FP32 early-exit path (tol, restart 20, extrapolated guess) against the
+    plain FP64 path (the reference's GMRES(50) full cycles, within 1e-9 of the
+    FP64 oracle) on the named configurations, over their whole runs, from
+    per-step device histories: activation times of every voxel (first and
+    re-activations) in units of dt, max |dVm| over the 1 kHz samples, and the
+    electrograms' relative L2 errors.
+
+    * c2: the rotor shell (Aliev-Panfilov, S1 plane + S2 quadrant, 1000 ms =
+      50,000 steps, 64 electrodes) at each wall thickness in ``walls``;
+    * c1: the 200 x 200 Mitchell-Schaeffer sheet, 500 ms, 16 electrodes (its
+      plain FP64 run against the FP64 oracle is
+      tests/test_gpu_configs.py::test_c1_sheet_full_run_matches_oracle);
+    * c3_sample: the ``c3_count`` smallest instances of the benchmark batch,
+      half Mitchell-Schaeffer and half Aliev-Panfilov, over their 500 ms."""
+    from pyheartsim_b200 import accuracy, workloads
+    out = {"reference": "plain FP64 path (GMRES(50) full cycles)", "test": f"FP32 early exit, tol {tol}"}
+    t0 = time.perf_counter()
+    case, pdur, el = workloads.sheet_c1()
+    out["c1"] = accuracy.compare_case(case, pdur, el, tol=tol)
+    out["c1"]["voxels"] = int(case[0])
+    for w in walls:
+        case, pdur, el = workloads.atrium_c2(wall=w)
+        r = accuracy.compare_case(case, pdur, el, tol=tol)
+        r["wall_voxels"] = int(w)
+        r["s1_s2_ms"] = workloads.C2_S1_S2_MS
+        out[f"c2_wall{w}"] = r
+    sizes = workloads.batch_sizes(64, 50_000, 400_000, 0)
+    picks = []
+    for model in (0, 1):
+        idx = [i for i in np.argsort(sizes) if i % 2 == model][:max(1, c3_count // 2)]
+        picks += [int(i) for i in idx]
+    sample = []
+    for i in picks:
+        _, case, meta = workloads.shell_case(i, int(sizes[i]), 0)
+        r = accuracy.compare_case(case, meta["pacing_ms"] / case[3]["time_scale"], tol=tol)
+        sample.append({"instance": i, "model": meta["model"], "voxels": int(case[0]),
+                       "first_max_dlat_steps": r["first"]["max_dlat_steps"] if r["first"] else None,
+                       "first_voxels_one_run_only": r["first"]["voxels_one_run_only"] if r["first"] else None,
+                       "reactivation_max_dlat_steps": max([x["max_dlat_steps"] or 0 for x in r["reactivations"]],
+                                                          default=None),
+                       "activation_count_equal_frac": r["activation_count_equal_frac"],
+                       "max_abs_dvm_1khz": r["max_abs_dvm_1khz"], "steps": r["steps"],
+                       "plain_fp64_s": r["plain_fp64_s"], "fast_fp32_s": r["fast_fp32_s"]})
+    out["c3_sample"] = sample
+    out["seconds"] = time.perf_counter() - t0
+    return out
 
 
 def serving_leg(args, plain_rate, dev, load=None, dur_ms=(200.0, 2000.0), count=None):
@@ -718,6 +832,12 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"geometry": geometry_leg(args, dev)}), flush=True)
+        return 0
+    if args.accuracy_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"accuracy": accuracy_leg(dev, args.tol, walls=tuple(args.c2_walls))}), flush=True)
         return 0
     if args.aniso_only:
         import torch

@@ -222,8 +222,11 @@ int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_p
  * Same inputs and result as phs_egm_contract_f64; its split-K partial sums live
  * in a fixed 16 MiB device array (phs_egm_noalloc_capacity() doubles) inside the
  * library, so T * n_e must not exceed that capacity (else PHS_ERR_BAD_ARG).  The
- * first call on a device looks up the array's address: make it before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race. */
+ * array's address is looked up on every call made outside a stream capture (so
+ * it stays valid after a device reset) and cached for calls made during one:
+ * make the first call on a device before any stream capture (else
+ * PHS_ERR_STATE).  All calls share the array, so calls that overlap on the GPU
+ * race. */
 int phs_egm_contract_f64_noalloc(int64_t T, int64_t n_v, int64_t n_e, const double* V, int64_t ldv,
                                  const double* Mt, double* egm, void* stream);
 int64_t phs_egm_noalloc_capacity(void);
@@ -302,6 +305,31 @@ int phs_operator_tables(phs_operator_tables_args* args);
  * first t maximising -(egm[t+1][e] - egm[t][e]) (NaN counts as the largest),
  * minus the minimum over electrodes.  egm [T][n_e], f64 (is_f64) or f32.      */
 int phs_electrode_lat(int64_t T, int64_t n_e, const void* egm, int is_f64, int32_t* lat_out, void* stream);
+/* utility/lat_map.py:29-46 (interpolate_lat) on the device: electrode LAT
+ * spread over voxels.  Inputs (device, f64): voxel [n_v][ndim] and electrode
+ * [n_e][ndim] coordinates with the constant dimensions already dropped (ndim 2
+ * or 3), lat_electrode [n_e], and the Delaunay triangulation of the electrodes
+ * as scipy.spatial.Delaunay gives it: simplices [n_simplex][ndim+1] (int32),
+ * transform [n_simplex][ndim+1][ndim] (inverse vertex matrix, then the last
+ * vertex), neighbors [n_simplex][ndim+1] (int32), min_bound/max_bound [ndim].
+ * Output lat_voxel [n_v]: barycentric interpolation in the first simplex (index
+ * order) containing the voxel within eps = 100 DBL_EPSILON, the nearest
+ * electrode's LAT outside the hull.  Asynchronous on `stream`.                */
+int phs_interpolate_lat(int64_t n_v, int ndim, const double* voxel, int64_t n_e, const double* electrode,
+                        const double* lat_electrode, int64_t n_simplex, const int32_t* simplices,
+                        const double* transform, const int32_t* neighbors, const double* min_bound,
+                        const double* max_bound, double* lat_voxel, void* stream);
+/* Every upward crossing of `threshold` by Vm, per voxel, in a device history
+ * hist [S][ld] (f64 or f32 per is_f64; e.g. phs_instance_device_ptrs' hist_u):
+ * sample s is a crossing when hist[s][v] >= threshold and hist[s-1][v] <
+ * threshold (the state before sample 0 counts as below).  The first
+ * max_per_voxel crossing samples of voxel v go to times[v*max_per_voxel + i]
+ * (device), counts[v] (device) gets the number of crossings.  The first
+ * crossing of a history sampled every step is the activation table of
+ * utility/lat_map.py's Vm counterpart (the step kernel's lat); the later ones
+ * are re-activations (re-entry).  Asynchronous on `stream`.                    */
+int phs_activation_times(int64_t S, int64_t n, const void* hist, int64_t ld, int is_f64, double threshold,
+                         int32_t max_per_voxel, int32_t* times, int32_t* counts, void* stream);
 /* Conduction velocity, utility/conduction_velocity.py:23-70: for each of n_e
  * points xyz [n_e][3] with activation times lat [n_e] (f64), the minimum-norm
  * least-squares plane through the points within `radius` (itself included;

@@ -9,6 +9,9 @@ Restates, in numpy/scipy, jiyuehe/PyHeartSim:
 * ``utility/lat_map.py:20-27``  compute_electrode_lat: argmax over time of the
   negative first difference of each electrode's signal, shifted so that the
   earliest electrode is 0;
+* ``utility/lat_map.py:29-46``  interpolate_lat: linear interpolation of the
+  electrode LAT over the voxels on the electrodes' Delaunay triangulation
+  (scipy), nearest electrode outside the hull;
 * ``utility/conduction_velocity.py:23-70``  compute: for every electrode, the
   electrodes within 8 mm (itself included), a least-squares plane
   ``lat = a x + b y + c z + d`` (numpy.linalg.lstsq, minimum-norm), velocity
@@ -57,3 +60,21 @@ def compute(simulation_results, geometry_data):
     lat = compute_electrode_lat(simulation_results['electrogram_unipolar'])
     xyz = geometry_data['voxel'][geometry_data['voxel_id_of_simulation_electrode'], :]
     return conduction_velocity(xyz, lat)
+
+
+def interpolate_lat(voxel, electrode_voxel, lat_electrode):
+    """utility/lat_map.py:29-46: drop the dimensions in which the electrodes do
+    not vary, interpolate linearly on the Delaunay triangulation of the
+    electrodes (scipy's LinearNDInterpolator, NaN outside the hull), and fill
+    the voxels outside the hull with the nearest electrode's value (scipy's
+    NearestNDInterpolator)."""
+    from scipy.interpolate import LinearNDInterpolator, NearestNDInterpolator
+    ev = np.asarray(electrode_voxel, dtype=np.float64)
+    vx = np.asarray(voxel, dtype=np.float64)
+    active = np.ptp(ev, axis=0) > 0
+    er, vr = ev[:, active], vx[:, active]
+    out = LinearNDInterpolator(er, lat_electrode)(vr)
+    nan = np.isnan(out)
+    if np.any(nan):
+        out[nan] = NearestNDInterpolator(er, lat_electrode)(vr[nan])
+    return out

@@ -187,6 +187,13 @@ SIGNATURES = {
                                          ctypes.c_void_p, ctypes.c_void_p]),
     "phs_conduction_velocity": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_interpolate_lat": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_activation_times": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                            ctypes.c_int, ctypes.c_double, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _lib = None

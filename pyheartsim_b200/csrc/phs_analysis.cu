@@ -13,10 +13,23 @@
 //                            SVD of the m x 4 system (one CTA per electrode);
 //                            velocity grad/|grad|^2, speed 1/|grad|, NaN with
 //                            fewer than 4 points or |grad|^2 <= 1e-8
+//   phs_interpolate_lat      utility/lat_map.py:29-46 -- electrode LAT spread
+//                            over the voxels: linear (barycentric) inside a
+//                            Delaunay triangulation of the electrodes, nearest
+//                            electrode outside its hull; the point location
+//                            follows scipy's LinearNDInterpolator rules (the
+//                            bounding-box test and the barycentric inside test
+//                            with eps = 100 DBL_EPSILON, degenerate simplices
+//                            through their neighbours with sqrt(DBL_EPSILON))
+//   phs_activation_times     every upward threshold crossing of Vm per voxel in
+//                            a [S][n] history (re-entry analysis: the first
+//                            crossing is the activation table the step kernel
+//                            records; the later ones are the re-activations)
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/phs.h"
@@ -74,6 +87,170 @@ __global__ void shift_to_zero(long long ne, int32_t* idx) {
     }
     const int mn = s[0];
     for (long long e = threadIdx.x; e < ne; e += blockDim.x) idx[e] -= mn;
+}
+
+// One thread per voxel, walking down the history (one coalesced row per
+// sample).  A crossing at sample s: u[s] >= thr and u[s-1] < thr, with the
+// state before sample 0 counted as below.  The first max_k crossing samples go
+// to times[v * max_k + i]; counts[v] is the number of crossings (it may exceed
+// max_k).
+template <typename T>
+__global__ void activation_kernel(long long S, long long n, const T* __restrict__ hist, long long ld, T thr, int max_k,
+                                  int32_t* __restrict__ times, int32_t* __restrict__ counts) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        bool above = false;
+        int c = 0;
+        for (long long s = 0; s < S; ++s) {
+            const bool a = hist[s * ld + v] >= thr;
+            if (a && !above) {
+                if (c < max_k) times[v * max_k + c] = (int32_t)s;
+                ++c;
+            }
+            above = a;
+        }
+        counts[v] = c;
+    }
+}
+
+// ---- interpolate_lat --------------------------------------------------------
+constexpr double kInterpEps = 100.0 * 2.220446049250313e-16;   // 100 DBL_EPSILON
+constexpr double kInterpEpsBroad = 1.4901161193847656e-08;     // sqrt(DBL_EPSILON)
+constexpr int kSimplexChunk = 64;
+
+// Barycentric coordinates of x in a simplex with transform tr (the inverse
+// vertex matrix [D][D] row-major, then the last vertex [D]): c[i] =
+// sum_j tr[D i + j] (x_j - r_j) for i < D, c[D] = 1 - c[0] - ... - c[D-1], each
+// an unfused multiply and add in that order (scipy's _barycentric_inside).
+template <int D>
+__device__ __forceinline__ void barycentric(const double* tr, const double* x, double* c) {
+    c[D] = 1.0;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+        double a = 0.0;
+#pragma unroll
+        for (int j = 0; j < D; ++j) a = __dadd_rn(a, __dmul_rn(tr[D * i + j], __dsub_rn(x[j], tr[D * D + j])));
+        c[i] = a;
+        c[D] = __dsub_rn(c[D], a);
+    }
+}
+
+template <int D>
+__device__ __forceinline__ bool inside_all(const double* c, double eps) {
+    bool in = true;
+#pragma unroll
+    for (int i = 0; i <= D; ++i) in = in && (-eps <= c[i]) && (c[i] <= 1.0 + eps);
+    return in;
+}
+
+// One thread per voxel: the first simplex (in index order) whose barycentric
+// coordinates all lie in [-eps, 1 + eps]; simplices with a NaN transform
+// (degenerate) are replaced by the test of their neighbours, with
+// sqrt(DBL_EPSILON) of leeway on the coordinate facing the degenerate one.
+// Value: sum_j c_j lat[vertex_j] in vertex order, or NaN outside (nearest
+// fallback in interp_nearest_kernel).
+template <int D>
+__global__ void interp_linear_kernel(long long nv, const double* __restrict__ pts, long long ns,
+                                     const int32_t* __restrict__ simplices, const double* __restrict__ transform,
+                                     const int32_t* __restrict__ neighbors, const double* __restrict__ lo,
+                                     const double* __restrict__ hi, const double* __restrict__ values,
+                                     double* __restrict__ out) {
+    constexpr int TS = D * (D + 1);
+    __shared__ double s_tr[kSimplexChunk * TS];
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool live = v < nv;
+    double x[D];
+    bool outside = !live;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        x[d] = live ? pts[v * D + d] : 0.0;
+        if (live && (x[d] < lo[d] - kInterpEps || x[d] > hi[d] + kInterpEps)) outside = true;
+    }
+    long long found = -1;
+    double cf[D + 1];
+#pragma unroll
+    for (int i = 0; i <= D; ++i) cf[i] = 0.0;
+    for (long long s0 = 0; s0 < ns; s0 += kSimplexChunk) {
+        const int cnt = (int)((ns - s0 < kSimplexChunk) ? ns - s0 : kSimplexChunk);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt * TS; i += blockDim.x) s_tr[i] = transform[s0 * TS + i];
+        __syncthreads();
+        if (outside || found >= 0) continue;
+        for (int q = 0; q < cnt && found < 0; ++q) {
+            const double* tr = s_tr + q * TS;
+            double c[D + 1];
+            if (tr[0] == tr[0]) {
+                barycentric<D>(tr, x, c);
+                if (inside_all<D>(c, kInterpEps)) {
+                    found = s0 + q;
+#pragma unroll
+                    for (int i = 0; i <= D; ++i) cf[i] = c[i];
+                }
+            } else {
+                const long long is = s0 + q;
+                for (int k = 0; k <= D && found < 0; ++k) {
+                    const int nbr = neighbors[is * (D + 1) + k];
+                    if (nbr < 0) continue;
+                    const double* tn = transform + (long long)nbr * TS;
+                    if (!(tn[0] == tn[0])) continue;
+                    barycentric<D>(tn, x, c);
+                    bool in = true;
+                    for (int m = 0; m <= D; ++m) {
+                        const double e = (neighbors[(long long)nbr * (D + 1) + m] == (int)is) ? kInterpEpsBroad
+                                                                                              : kInterpEps;
+                        in = in && (-e <= c[m]) && (c[m] <= 1.0 + kInterpEps);
+                    }
+                    if (in) {
+                        found = nbr;
+#pragma unroll
+                        for (int i = 0; i <= D; ++i) cf[i] = c[i];
+                    }
+                }
+            }
+        }
+    }
+    if (!live) return;
+    if (found < 0) {
+        out[v] = __longlong_as_double(0x7ff8000000000000ll);   // NaN: outside the hull
+        return;
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j <= D; ++j) acc = __dadd_rn(acc, __dmul_rn(cf[j], values[simplices[found * (D + 1) + j]]));
+    out[v] = acc;
+}
+
+// Nearest electrode of every voxel whose linear value is NaN: the smallest
+// squared distance, summed over the dimensions in order; the lowest index on
+// an exact tie.
+template <int D>
+__global__ void interp_nearest_kernel(long long nv, const double* __restrict__ pts, long long ne,
+                                      const double* __restrict__ epts, const double* __restrict__ values,
+                                      double* __restrict__ out) {
+    __shared__ double s_e[kSimplexChunk * D];
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool need = v < nv && isnan(out[v]);
+    double x[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = need ? pts[v * D + d] : 0.0;
+    double best = 0.0;
+    long long bi = -1;
+    for (long long e0 = 0; e0 < ne; e0 += kSimplexChunk) {
+        const int cnt = (int)((ne - e0 < kSimplexChunk) ? ne - e0 : kSimplexChunk);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt * D; i += blockDim.x) s_e[i] = epts[e0 * D + i];
+        __syncthreads();
+        if (!need) continue;
+        for (int q = 0; q < cnt; ++q) {
+            double d2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const double t = __dsub_rn(x[d], s_e[q * D + d]);
+                d2 = __dadd_rn(d2, __dmul_rn(t, t));
+            }
+            if (bi < 0 || d2 < best) { best = d2; bi = e0 + q; }
+        }
+    }
+    if (need && bi >= 0) out[v] = values[bi];
 }
 
 // squared distance in the order scipy's cKDTree accumulates it (x, y, z)
@@ -243,6 +420,46 @@ int phs_electrode_lat(int64_t nt, int64_t ne, const void* egm, int is_f64, int32
     shift_to_zero<<<1, kAThreads, 0, s>>>(ne, lat_out);
     PHS_CUDA_TRY(cudaGetLastError());
     PHS_CUDA_TRY(cudaStreamSynchronize(s));
+    return PHS_OK;
+}
+
+int phs_interpolate_lat(int64_t n_v, int ndim, const double* voxel, int64_t n_e, const double* electrode,
+                        const double* lat_electrode, int64_t n_simplex, const int32_t* simplices,
+                        const double* transform, const int32_t* neighbors, const double* min_bound,
+                        const double* max_bound, double* lat_voxel, void* stream) {
+    if (n_v <= 0 || n_e <= 0 || n_simplex <= 0 || (ndim != 2 && ndim != 3) || !voxel || !electrode ||
+        !lat_electrode || !simplices || !transform || !neighbors || !min_bound || !max_bound || !lat_voxel)
+        return PHS_ERR_BAD_ARG;
+    if (n_v > 65535LL * 128) return PHS_ERR_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned int blocks = (unsigned int)((n_v + 127) / 128);
+    if (ndim == 2) {
+        interp_linear_kernel<2><<<blocks, 128, 0, s>>>(n_v, voxel, n_simplex, simplices, transform, neighbors,
+                                                       min_bound, max_bound, lat_electrode, lat_voxel);
+        interp_nearest_kernel<2><<<blocks, 128, 0, s>>>(n_v, voxel, n_e, electrode, lat_electrode, lat_voxel);
+    } else {
+        interp_linear_kernel<3><<<blocks, 128, 0, s>>>(n_v, voxel, n_simplex, simplices, transform, neighbors,
+                                                       min_bound, max_bound, lat_electrode, lat_voxel);
+        interp_nearest_kernel<3><<<blocks, 128, 0, s>>>(n_v, voxel, n_e, electrode, lat_electrode, lat_voxel);
+    }
+    PHS_CUDA_TRY(cudaGetLastError());
+    return PHS_OK;
+}
+
+int phs_activation_times(int64_t S, int64_t n, const void* hist, int64_t ld, int is_f64, double threshold,
+                         int32_t max_per_voxel, int32_t* times, int32_t* counts, void* stream) {
+    if (S <= 0 || n <= 0 || ld < n || S > INT32_MAX || max_per_voxel < 0 || !hist || !counts ||
+        (max_per_voxel > 0 && !times))
+        return PHS_ERR_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned int blocks = (unsigned int)std::min<long long>((n + 255) / 256, 65535);
+    if (is_f64)
+        activation_kernel<double><<<blocks, 256, 0, s>>>(S, n, (const double*)hist, ld, threshold, max_per_voxel,
+                                                         times, counts);
+    else
+        activation_kernel<float><<<blocks, 256, 0, s>>>(S, n, (const float*)hist, ld, (float)threshold,
+                                                        max_per_voxel, times, counts);
+    PHS_CUDA_TRY(cudaGetLastError());
     return PHS_OK;
 }
 

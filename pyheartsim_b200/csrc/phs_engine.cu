@@ -483,23 +483,27 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     // ---- leader bodies ------------------------------------------------------
     // Deterministic sums of partial slots slot0 .. slot0+ns-1 over all tiles, by
     // the whole leader CTA: thread t adds partials t, t+256, ... in order (four
-    // slots per pass, their loads issued together), then a fixed xor tree per
+    // or eight slots per pass, their loads issued together), then a fixed xor tree per
     // warp and the warp results in warp order.  The order depends only on the
     // partial count, not on the team size.  Results in bsum_out[0..ns).
     __shared__ double bsum_w[kMaxRestart + 1][kWarps];
     __shared__ double bsum_out[kMaxRestart + 1];
+    // FP64 (one partial per tile, long GMRES(50) cycles): eight slots per pass
+    constexpr int kSumW = sizeof(T) == 8 ? 8 : 4;
     auto block_sum = [&](int slot0, int ns) {
-        for (int s0 = 0; s0 < ns; s0 += 4) {
-            double a[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int s0 = 0; s0 < ns; s0 += kSumW) {
+            double a[kSumW];
+#pragma unroll
+            for (int u = 0; u < kSumW; ++u) a[u] = 0.0;
 #pragma unroll 4
             for (int q = threadIdx.x; q < nparts; q += kThreads) {
                 const double* pq = I.part + (size_t)q * ps + slot0 + s0;
 #pragma unroll
-                for (int u = 0; u < 4; ++u)
+                for (int u = 0; u < kSumW; ++u)
                     if (s0 + u < ns) a[u] += __ldcg(pq + u);
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kSumW; ++u) {
                 const double v = warp_sum(a[u]);
                 if (lane == 0 && s0 + u < ns) bsum_w[s0 + u][warp] = v;
             }
@@ -564,73 +568,95 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
     };
 
+    // Givens update of Hessenberg column j and, when the cycle ends, the back
+    // substitution R y = g.  The rotations, the column, g, s and (at a cycle
+    // end) the k x k triangle of R are first loaded into shared memory by the
+    // whole CTA, so the sequential parts run on shared memory instead of a
+    // chain of dependent L2 round trips; the arithmetic and its order are
+    // those of a plain sequential Givens QR.
+    __shared__ double gv_cs[kMaxRestart], gv_sn[kMaxRestart], gv_col[kMaxRestart + 2];
+    __shared__ double gv_g[kMaxRestart + 1], gv_s[kMaxRestart + 1], gv_y[kMaxRestart + 1];
+    __shared__ double gv_R[kMaxRestart * (kMaxRestart + 1) / 2];   // column l, rows 0..l at l(l+1)/2 + i
+    __shared__ int gv_act;
     auto leader_norm = [&](int j) {
         block_sum(0, 1);
-        if (warp == 0) {
-            double u2 = bsum_out[0];
-            if (lane == 0) {
-                double* Rc = sc->R + j * (kMaxRestart + 1);
-                double hn = sqrt(u2);
-                Rc[j + 1] = hn;
-                // apply the previous rotations to column j
-                for (int i = 0; i < j; ++i) {
-                    double c = sc->cs[i], s = sc->sn[i];
-                    double a = Rc[i], bb = Rc[i + 1];
-                    Rc[i] = c * a + s * bb;
-                    Rc[i + 1] = -s * a + c * bb;
-                }
-                double a = Rc[j], bb = Rc[j + 1];
-                double r = hypot(a, bb);
-                double c = (r == 0.0) ? 1.0 : a / r;
-                double s = (r == 0.0) ? 0.0 : bb / r;
-                sc->cs[j] = c;
-                sc->sn[j] = s;
-                Rc[j] = r;
-                Rc[j + 1] = 0.0;
-                double gj = sc->g[j];
-                sc->g[j] = c * gj;
-                sc->g[j + 1] = -s * gj;
-                double est = fabs(sc->g[j + 1]);
-                sc->est = est;
-                sc->iters_solve += 1;
-                int act;
-                bool finite = isfinite(hn) && isfinite(r);
-                bool breakdown = (hn == 0.0);
-                bool conv = (!I.full_cycles) && (est <= sc->atol_eff);
-                if (!finite) {
-                    act = ACT_FAIL;
-                    I.st->status = PHS_ERR_NONFINITE;
-                } else if (conv || (breakdown && !I.full_cycles)) {
-                    act = ACT_UPDATE_FINAL;
-                } else if (j + 1 >= I.m || breakdown) {
-                    act = ACT_UPDATE_CHECK;
-                } else {
-                    act = ACT_NEXT_J;
-                    sc->s[j + 1] = 1.0 / hn;
-                }
-                if (act == ACT_UPDATE_FINAL || act == ACT_UPDATE_CHECK) sc->k = j + 1;
-                if (act == ACT_UPDATE_FINAL) account_solve();
-                sc->action = act;
-            }
+        double* Rc = sc->R + j * (kMaxRestart + 1);
+        for (int i = threadIdx.x; i < j; i += kThreads) {
+            gv_cs[i] = __ldcg(sc->cs + i);
+            gv_sn[i] = __ldcg(sc->sn + i);
+        }
+        for (int i = threadIdx.x; i <= j; i += kThreads) {
+            gv_col[i] = __ldcg(Rc + i);
+            gv_g[i] = __ldcg(sc->g + i);
+            gv_s[i] = __ldcg(sc->s + i);
         }
         __syncthreads();
-        // back substitution R y = g (k x k upper triangular), one warp
-        if (warp == 0) {
-            int act = sc->action;
-            if (act == ACT_UPDATE_FINAL || act == ACT_UPDATE_CHECK) {
-                int k = sc->k;
-                for (int i = k - 1; i >= 0; --i) {
-                    double acc = 0.0;
-                    for (int l = i + 1 + lane; l < k; l += 32)
-                        acc += sc->R[l * (kMaxRestart + 1) + i] * sc->coef[l];
-                    acc = warp_sum(acc);
-                    if (lane == 0) sc->coef[i] = (sc->g[i] - acc) / sc->R[i * (kMaxRestart + 1) + i];
-                    __syncwarp();
-                }
-                __syncwarp();
-                // scale: x += sum_j y_j v_j = sum_j (y_j s_j) V_j
-                for (int i = lane; i < k; i += 32) sc->coef[i] *= sc->s[i];
+        if (threadIdx.x == 0) {
+            const double hn = sqrt(bsum_out[0]);
+            gv_col[j + 1] = hn;
+            // apply the previous rotations to column j
+            for (int i = 0; i < j; ++i) {
+                const double c = gv_cs[i], s = gv_sn[i];
+                const double a = gv_col[i], bb = gv_col[i + 1];
+                gv_col[i] = c * a + s * bb;
+                gv_col[i + 1] = -s * a + c * bb;
             }
+            const double a = gv_col[j], bb = gv_col[j + 1];
+            const double r = hypot(a, bb);
+            const double c = (r == 0.0) ? 1.0 : a / r;
+            const double s = (r == 0.0) ? 0.0 : bb / r;
+            sc->cs[j] = c;
+            sc->sn[j] = s;
+            gv_col[j] = r;
+            gv_col[j + 1] = 0.0;
+            const double gj = gv_g[j];
+            gv_g[j] = c * gj;
+            gv_g[j + 1] = -s * gj;
+            sc->g[j] = gv_g[j];
+            sc->g[j + 1] = gv_g[j + 1];
+            const double est = fabs(gv_g[j + 1]);
+            sc->est = est;
+            sc->iters_solve += 1;
+            int act;
+            const bool finite = isfinite(hn) && isfinite(r);
+            const bool breakdown = (hn == 0.0);
+            const bool conv = (!I.full_cycles) && (est <= sc->atol_eff);
+            if (!finite) {
+                act = ACT_FAIL;
+                I.st->status = PHS_ERR_NONFINITE;
+            } else if (conv || (breakdown && !I.full_cycles)) {
+                act = ACT_UPDATE_FINAL;
+            } else if (j + 1 >= I.m || breakdown) {
+                act = ACT_UPDATE_CHECK;
+            } else {
+                act = ACT_NEXT_J;
+                sc->s[j + 1] = 1.0 / hn;
+            }
+            if (act == ACT_UPDATE_FINAL || act == ACT_UPDATE_CHECK) sc->k = j + 1;
+            if (act == ACT_UPDATE_FINAL) account_solve();
+            sc->action = act;
+            gv_act = act;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i <= j + 1; i += kThreads) Rc[i] = gv_col[i];
+        const int act = gv_act;
+        if (act != ACT_UPDATE_FINAL && act != ACT_UPDATE_CHECK) return;
+        // back substitution R y = g (k x k upper triangular), k = j + 1
+        const int k = j + 1;
+        for (int l = warp; l < k; l += kWarps)
+            for (int i = lane; i <= l; i += 32)
+                gv_R[l * (l + 1) / 2 + i] = (l == j) ? gv_col[i] : __ldcg(sc->R + l * (kMaxRestart + 1) + i);
+        __syncthreads();
+        if (warp == 0) {
+            for (int i = k - 1; i >= 0; --i) {
+                double acc = 0.0;
+                for (int l = i + 1 + lane; l < k; l += 32) acc += gv_R[l * (l + 1) / 2 + i] * gv_y[l];
+                acc = warp_sum(acc);
+                if (lane == 0) gv_y[i] = (gv_g[i] - acc) / gv_R[i * (i + 1) / 2 + i];
+                __syncwarp();
+            }
+            // scale: x += sum_j y_j v_j = sum_j (y_j s_j) V_j
+            for (int i = lane; i < k; i += 32) sc->coef[i] = gv_y[i] * gv_s[i];
         }
     };
 

@@ -21,9 +21,12 @@
 //   * the array keeps the previous call's contents; nothing in it needs to
 //     start at zero, because every partial a call reads is first written by the
 //     same call.
-// The first call on each device looks up the array's device address
-// (cudaGetSymbolAddress) with that device current and caches it; make that
-// first call before any stream capture.
+// The array's device address is looked up (cudaGetSymbolAddress) with the
+// calling device current.  Outside a stream capture the lookup is repeated on
+// every call, so the address stays right after a device reset reloads the
+// module; during a capture the address cached by the last call made outside a
+// capture is used.  Make the first call on each device before any stream
+// capture.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -46,14 +49,28 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_addr[kMaxDevices] = {};
 
-// Device address of g_noalloc_partials on the current device (looked up once).
-int noalloc_partials(double** out) {
+// Device address of g_noalloc_partials on the current device: looked up again
+// when `stream` is not capturing, the cached address while it is.
+int noalloc_partials(cudaStream_t stream, double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { set_last_error("phs_egm_contract_f64_noalloc: cudaGetDevice", e); return PHS_ERR_CUDA; }
-    if (dev < 0 || dev >= kMaxDevices) return PHS_ERR_UNSUPPORTED;
+    if (dev < 0 || dev >= kMaxDevices) {
+        char msg[128];
+        snprintf(msg, sizeof(msg), "phs_egm_contract_f64_noalloc: device %d is beyond the %d devices it serves", dev,
+                 kMaxDevices);
+        set_last_message(msg);
+        return PHS_ERR_UNSUPPORTED;
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(stream, &cap);
+    if (e != cudaSuccess) { set_last_error("phs_egm_contract_f64_noalloc: cudaStreamIsCapturing", e); return PHS_ERR_CUDA; }
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_noalloc_addr[dev]) {
+        if (cap != cudaStreamCaptureStatusNone) {
+            set_last_message("phs_egm_contract_f64_noalloc: first call on this device made during a stream capture");
+            return PHS_ERR_STATE;
+        }
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_partials);
         if (e != cudaSuccess) {
@@ -85,7 +102,7 @@ int phs_egm_contract_f64_noalloc(int64_t T, int64_t n_v, int64_t n_e, const doub
         return PHS_ERR_BAD_ARG;
     }
     double* partials = nullptr;
-    int rc = phs::noalloc_partials(&partials);
+    int rc = phs::noalloc_partials((cudaStream_t)stream, &partials);
     if (rc != PHS_OK) return rc;
     return phs::contract_f64_into(T, n_v, n_e, V, ldv, Mt, egm, partials, phs::kNoAllocPartials,
                                   (cudaStream_t)stream);

@@ -78,6 +78,43 @@ class BatchedEngine:
             return u, inst.to_caller(h)
         return u
 
+    def activation_times(self, slot, max_per_voxel=16, threshold=0.5, stream=None):
+        """Every upward crossing of ``threshold`` by Vm in the instance's device
+        history (``phs_activation_times``): ``(times, counts)`` in the caller's
+        voxel order, ``times[v, i]`` the sample index of crossing i of voxel v
+        (-1 past ``counts[v]``).  With a history sampled every step
+        (``sample_stride`` 1) the first crossing is the activation step and the
+        later ones are the re-activations, in units of dt."""
+        import torch
+        inst = self._inst[slot]
+        info = self.info(slot)
+        u = ctypes.c_void_p()
+        hist = ctypes.c_void_p()
+        lat = _lib.c_int32_p()
+        _lib.check(_lib.lib().phs_instance_device_ptrs(self._h, slot, ctypes.byref(u), ctypes.byref(hist),
+                                                       ctypes.byref(lat)), "phs_instance_device_ptrs")
+        n = int(inst.n_voxel)
+        S = int(info["samples"])
+        dev = torch.device("cuda", torch.cuda.current_device())
+        times = torch.full((n, max(int(max_per_voxel), 1)), -1, dtype=torch.int32, device=dev)
+        counts = torch.zeros(n, dtype=torch.int32, device=dev)
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        torch.cuda.synchronize(dev)
+        _lib.check(_lib.lib().phs_activation_times(S, n, hist, n, int(self.precision == _lib.PREC_F64),
+                                                   float(threshold), int(max_per_voxel),
+                                                   ctypes.c_void_p(times.data_ptr()),
+                                                   ctypes.c_void_p(counts.data_ptr()), ctypes.c_void_p(stream)),
+                   "phs_activation_times")
+        torch.cuda.synchronize(dev)
+        t = times.cpu().numpy()[:, :int(max_per_voxel)]
+        c = counts.cpu().numpy()
+        if inst.inv is not None:
+            t, c = t[inst.inv], c[inst.inv]
+        return t, c
+
     def state(self, slot):
         inst = self._inst[slot]
         dt = _lib.np_dtype(self.precision)

@@ -166,6 +166,33 @@ class DeviceInstance(CompiledInstance):
                     nb_edge=g(self.nb_edge_t), coef_edge=g(self.coef_edge_t))
 
 
+def compile_reference_inputs(n_voxel, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters, *,
+                             reorder=True, stream=None, **kw):
+    """The drop-in's own inputs (``n_voxel``, ``P_2d`` (n, 21), ``geometry_data``
+    with ``neighbor_id_2d`` (n, 18) and ``Delta``, optionally ``voxel`` (n, 3) in
+    mm for the row order, and the two parameter dicts of
+    simulation/simulation_gpu.py:261) -> a :class:`DeviceInstance` whose
+    operator tables are compiled on the GPU from the uploaded P_2d and
+    neighbour table.  Same tables, order and scalars as
+    :func:`pyheartsim_b200.instance.compile_instance` (the host compiler)."""
+    torch = _torch()
+    n = int(n_voxel)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    P = torch.as_tensor(np.ascontiguousarray(np.asarray(P_2d, dtype=np.float64)), device=dev)
+    nb18 = torch.as_tensor(np.ascontiguousarray(np.asarray(geometry_data['neighbor_id_2d'], dtype=np.int32)),
+                           device=dev)
+    if P.shape != (n, 21) or nb18.shape != (n, 18):
+        raise ValueError("P_2d must be (n_voxel, 21) and neighbor_id_2d (n_voxel, 18)")
+    order = None
+    vox = geometry_data.get('voxel') if hasattr(geometry_data, 'get') else None
+    if reorder and vox is not None and np.shape(vox) == (n, 3):
+        ijk = torch.round(torch.as_tensor(np.asarray(vox, dtype=np.float64), device=dev)
+                          / float(geometry_data['Delta'])).to(torch.int32)
+        _, order = lattice_neighbors(ijk, order=True, stream=stream)
+    return _compile_tables(n, P, nb18, order, float(geometry_data['Delta']), simulation_parameters,
+                           arrhythmia_parameters, stream, dev, **kw)
+
+
 def compile_instance(voxel, Delta, parameter, D0, simulation_parameters, arrhythmia_parameters, *,
                      reorder=True, stream=None, **kw):
     """Voxel coordinates (n, 3) in mm and per-voxel parameters (the reference's
@@ -180,6 +207,14 @@ def compile_instance(voxel, Delta, parameter, D0, simulation_parameters, arrhyth
     ijk = torch.round(torch.as_tensor(vox, device=dev) / float(Delta)).to(torch.int32)
     nb18, order = lattice_neighbors(ijk, order=bool(reorder), stream=stream)
     P = equation_parts(simulation_parameters, nb18, D0, parameter, stream=stream)
+    return _compile_tables(n, P, nb18, order, float(Delta), simulation_parameters, arrhythmia_parameters, stream,
+                           dev, **kw)
+
+
+def _compile_tables(n, P, nb18, order, Delta, simulation_parameters, arrhythmia_parameters, stream, dev, **kw):
+    """Operator tables of an instance from device P_2d, neighbour table and row
+    order (``phs_operator_flags``, ``phs_operator_tables``)."""
+    torch = _torch()
     sc, s1, s2 = instance_scalars(simulation_parameters, arrhythmia_parameters, **kw)
     node_flag = np.asarray(arrhythmia_parameters['node_flag'])
     sc["tblock_steps"] = tblock_steps(sc["n_steps"], sc["dt"]) if np.any(node_flag == 3) else 0

@@ -20,6 +20,10 @@ A solve with k Arnoldi steps therefore costs
 e.g. 90 + 68 k + 4 k^2 bytes in FP32 with six stored coefficients, and
 71 + 49 k + 4 k^2 with isotropic rows.
 
+The plain form (GMRES(50) full cycles) also runs the true-residual test at the
+end of every cycle: read x, b, nb, coefficients; write V0 and u = 4 s + 24 + cb
+per cycle.
+
 Anisotropic rows (edge cross terms) add the edge table, 12 int32 indices and
 six coefficients = 48 + 6 s, to every operator application (the RHS stencil
 and each A_j): in FP32 +72 bytes per step and +72 per Arnoldi step.
@@ -38,14 +42,16 @@ def edge_bytes(s):
     return 48 + 6 * s
 
 
-def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False, edge=False):
+def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False, edge=False,
+                      checks=0):
     """Total algorithmic bytes of ``steps`` steps of an instance with ``voxels``
     voxels whose solves took ``k_sum`` Arnoldi steps in total (``k_sq_sum`` =
     sum of squares).  Steps that needed no iteration still run the RHS phase
-    and the final copy (2 s)."""
+    and the final copy (2 s).  ``checks``: true-residual tests at cycle ends
+    (full cycles)."""
     cb = coef_bytes(s, iso)
     per_voxel = (steps * (bytes_rhs(s, cb) + 2 * s) + (5 * s + 24 + cb) * k_sum + s * (k_sq_sum - k_sum)
-                 + s * k_sum)
+                 + s * k_sum + checks * (4 * s + 24 + cb))
     if guess:     # read the increment in the RHS phase; read and rewrite it in the final update
         per_voxel += steps * s + 2 * s * (solves or 0)
     if edge:

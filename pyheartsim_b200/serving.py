@@ -9,10 +9,12 @@ between launches,
 * advances every admitted instance by ``steps_per_launch`` steps in one
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
-* retires instances that reached their last step: reads the 1 kHz Vm history
-  back, frees their device memory and lets the next request in;
+* retires instances that reached their last step: reads the whole 1 kHz Vm
+  history back to the host (a request's latency ends when its history is
+  there), frees their device memory and lets the next request in;
 * re-splits CTAs over the running instances by measured cost every
-  ``rebalance_every`` launches.
+  ``rebalance_every`` launches (the device phase timers run only in the launch
+  before each re-split).
 
 Request inputs are compiled on host threads while the GPU runs.  Because the
 engine's reductions do not depend on team size or batch-mates, every result is
@@ -44,6 +46,7 @@ class Request:
         self.done_s = None
         self.slot = None
         self.history = None
+        self.history_bytes = 0
         self.status = None
 
 
@@ -114,7 +117,6 @@ class Server:
         self.builder = builder or (lambda r: build(r, self.tol, device=device_build))
         self.footprint = footprint or footprint_bytes
         self.engine = engine if engine is not None else BatchedEngine(_lib.PREC_F32)
-        self.engine.set_profile(True)
         self.pool = ThreadPoolExecutor(max_workers=build_threads) if build_threads > 0 else _Inline()
         self.stream = stream
         self.used = 0
@@ -161,18 +163,22 @@ class Server:
                 if nxt < len(reqs):
                     time.sleep(max(0.0, min(0.05, reqs[nxt].arrival_s * time_scale - now)))
                 continue
+            # phase timers only for the launch whose costs the next re-split uses
+            due = (self.launches + 1) % self.rebalance_every == 0
+            if due:
+                self.engine.set_profile(True)
             self.engine.advance(self.S, stream=self.stream, sync=True)
             self.launches += 1
-            if self.launches % self.rebalance_every == 0:
+            if due:
                 self.engine.rebalance()
+                self.engine.set_profile(False)
             for slot in list(active):
                 info = self.engine.info(slot)
                 if info["step"] >= info["n_steps"] or info["status"] == _lib.PHS_ERR_NONFINITE:
                     r = active.pop(slot)
-                    if keep_history:
-                        r.history = self.engine.history(slot)
-                    else:
-                        self.engine.history(slot, count=min(info["samples"], 1))   # results leave the device
+                    hist = self.engine.history(slot)           # the whole 1 kHz Vm history, to the host
+                    r.history_bytes = hist.nbytes
+                    r.history = hist if keep_history else None
                     r.status = info["status"]
                     r.done_s = time.perf_counter() - t0
                     work += float(r.inst.n_voxel) * info["step"]
@@ -194,7 +200,9 @@ def summarize(done, totals, requests, time_scale=1.0):
     wait = np.array([r.admit_s - r.arrival_s * time_scale for r in done])
     span = max(r.arrival_s for r in requests) * time_scale if requests else 0.0
     offered = sum(r.inst.n_voxel * r.inst.n_steps for r in done) / max(span, 1e-9)
-    return {"requests": len(done), "p50_latency_s": float(np.percentile(lat, 50)),
+    return {"requests": len(done), "latency_to": "the whole 1 kHz Vm history on the host",
+            "history_bytes": int(sum(r.history_bytes for r in done)),
+            "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "p50_queue_s": float(np.percentile(wait, 50)),
             "throughput_voxel_steps_s": totals["voxel_steps"] / totals["makespan_s"],
             "offered_voxel_steps_s": offered, "makespan_s": totals["makespan_s"],

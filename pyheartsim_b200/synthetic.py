@@ -190,3 +190,19 @@ def electrodes_off_surface(ijk, Delta, n_e, rng, offset=2.0):
     d = xyz[idx] - ctr
     d /= np.maximum(np.linalg.norm(d, axis=1, keepdims=True), 1e-12)
     return xyz[idx] + offset * d
+
+
+def small_shell_case(seed=1, t_phys=40.0, dt=0.05, scar_cov=0.15, fibres=False):
+    """A small scarred Mitchell-Schaeffer shell (semi-axes 9/8/7 mm, wall 3
+    voxels, two vein holes, ~12k voxels) paced at one seeded healthy site:
+    ((n, P_2d, geometry_data, simulation_parameters, arrhythmia_parameters),
+    pacing_ms).  ``fibres``: rule-based fibre field (anisotropic D0)."""
+    ijk = shell((9.0, 8.0, 7.0), 0.4, 3, 2, 2.0, seed)
+    rng = np.random.default_rng(seed)
+    nb = lattice_neighbors(ijk)
+    c = scar(ijk, nb, scar_cov, rng)
+    healthy = np.where(c == 1.0)[0]
+    centre = ijk[healthy[int(rng.integers(0, healthy.size))]]
+    s1 = np.where(np.sum((ijk - centre) ** 2, axis=1) <= 9)[0]
+    D0 = fibre_tensors(ijk) if fibres else None
+    return make_case(ijk, 0.4, 0, dt, t_phys, s1, flag=4, c_scale=c, D0=D0), 2.0

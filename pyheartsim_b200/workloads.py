@@ -30,10 +30,10 @@ def _shell_scaled(n_target, seed, Delta=0.4, wall=3):
     return synthetic.shell(tuple(np.asarray(base) * s), Delta, wall, 4, 5.0 * s, seed)
 
 
-def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-5, restart=20,
-               save_h=False, pacing_ms=2.0, fibres=False):
-    """Reference-style inputs + the compiled instance of shell ``i`` (``fibres``:
-    rule-based fibre field, anisotropic D0)."""
+def shell_inputs(i, n_target, seed, t_phys=500.0, scar_max=0.3, pacing_ms=2.0, fibres=False):
+    """Reference-style inputs of shell ``i``: ((n_voxel, P_2d, geometry_data,
+    simulation_parameters, arrhythmia_parameters), meta); ``fibres``:
+    rule-based fibre field, anisotropic D0."""
     rng = np.random.default_rng(seed * 1000 + i)
     ijk = _shell_scaled(n_target, seed * 1000 + i)
     nb = lattice_neighbors(ijk)
@@ -46,11 +46,19 @@ def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-
     dt_phys = 0.05 if model == 0 else 0.02
     D0 = synthetic.fibre_tensors(ijk) if fibres else None
     n, P, geom, sp, ap = synthetic.make_case(ijk, 0.4, model, dt_phys, t_phys, s1, flag=4, c_scale=c_scale, D0=D0)
+    return (n, P, geom, sp, ap), {"index": i, "n": n, "model": model, "scar": cov, "pacing_ms": pacing_ms,
+                                  "fibres": bool(fibres)}
+
+
+def shell_case(i, n_target, seed, t_phys=500.0, scar_max=0.3, fast=True, tol=1e-5, restart=20,
+               save_h=False, pacing_ms=2.0, fibres=False):
+    """Reference-style inputs + the compiled instance of shell ``i`` (``fibres``:
+    rule-based fibre field, anisotropic D0)."""
+    (n, P, geom, sp, ap), meta = shell_inputs(i, n_target, seed, t_phys, scar_max, pacing_ms, fibres)
     inst = _instance.compile_instance(n, P, geom, sp, ap, full_cycles=not fast, tol=tol, atol=1e-5,
                                       restart=restart if fast else 50, pacing_duration=pacing_ms / sp['time_scale'],
                                       save_h=save_h)
-    return inst, (n, P, geom, sp, ap), {"index": i, "n": n, "model": model, "scar": cov,
-                                        "pacing_ms": pacing_ms, "fibres": bool(fibres)}
+    return inst, (n, P, geom, sp, ap), meta
 
 
 def shell_case_device(i, n_target, seed, t_phys=500.0, scar_max=0.3, tol=1e-5, restart=20, save_h=False,
@@ -86,6 +94,24 @@ def _build_one(args):
     return inst, meta
 
 
+def _inputs_one(args):
+    i, n_target, seed, kw = args
+    return shell_inputs(i, n_target, seed, **kw)
+
+
+def batched_inputs(count=64, n_min=50_000, n_max=400_000, seed=0, workers=None, **kw):
+    """List of (reference-style inputs, meta) of the batched configuration,
+    uncompiled (for the drop-in's end-to-end path)."""
+    sizes = batch_sizes(count, n_min, n_max, seed)
+    jobs = [(i, int(sizes[i]), seed, kw) for i in range(count)]
+    workers = workers or min(count, max(1, (os.cpu_count() or 2) - 1), 32)
+    if workers <= 1 or count <= 1:
+        return [_inputs_one(j) for j in jobs]
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        return list(ex.map(_inputs_one, jobs))
+
+
 def batch_sizes(count, n_min, n_max, seed):
     rng = np.random.default_rng(seed)
     return np.exp(rng.uniform(np.log(n_min), np.log(n_max), size=count)).astype(np.int64)
@@ -101,3 +127,50 @@ def batched_shells(count=64, n_min=50_000, n_max=400_000, seed=0, workers=None, 
     ctx = mp.get_context("spawn")
     with ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
         return list(ex.map(_build_one, jobs))
+
+
+# ----------------------------------------------------------------- named accuracy configurations
+
+def sheet_c1(nx=200, ny=200, t_phys=500.0):
+    """The plain FP64 sheet: nx x ny voxels (Delta 0.4 mm, c = 1, isotropic),
+    Mitchell-Schaeffer (tau_in 0.3, tau_out 6, tau_open 120, tau_close 150,
+    v_gate 0.13), dt 0.05 ms, a 5 x 5 corner stimulus at t = 0 lasting 1 ms
+    (arrhythmia_flag 4), ``t_phys`` ms (10,000 steps at 500 ms), and 16
+    electrodes on a 4 x 4 grid 1 mm above the sheet.
+    Returns ((n, P_2d, geometry_data, simulation_parameters,
+    arrhythmia_parameters), pacing_ms, electrode_xyz)."""
+    ijk = synthetic.sheet(nx, ny)
+    s1 = np.where((ijk[:, 0] < 5) & (ijk[:, 1] < 5))[0]
+    case = synthetic.make_case(ijk, 0.4, 0, 0.05, t_phys, s1, flag=4)
+    return case, 1.0, synthetic.electrodes_grid(nx, ny, 0.4)
+
+
+# S1-S2 coupling interval of the rotor shell, in physical ms.  Chosen by a sweep
+# of the FP32 engine over 120-330 ms (wall 3 and wall 8): the shortest interval
+# whose S2 wave still propagates, which leaves re-entrant activity running to
+# the end of the 1000 ms run on both walls.
+C2_S1_S2_MS = 0.0
+
+
+def atrium_c2(wall=3, seed=0, t_phys=1000.0, s1_s2=None, n_electrodes=64):
+    """The rotor shell: ellipsoidal shell with semi-axes 25/20/18 mm (Delta 0.4
+    mm, ``wall`` voxels thick: 91,292 voxels at wall 3, 218,403 at wall 8) with
+    four r = 5 mm vein holes along seeded radial directions; Aliev-Panfilov
+    (k 8, a 0.15, eps0 0.002, mu1 0.2, mu2 0.3) with the reference's time
+    scaling (time_scale 6, c = 1.6 x 6, configuration.py:141-157); dt 0.02 ms
+    physical (0.02/6 model), ``t_phys`` ms (50,000 steps at 1000 ms).  S1: the
+    plane of voxels within 1.2 mm of the lowest x, at t = 0; S2: the quadrant
+    x < 0, y > 0 (the shell is centred on the origin) ``s1_s2`` ms later
+    (arrhythmia_flag 1, the reference's 5 ms stimuli); 64 electrodes 2 mm off
+    the surface at seeded voxels.
+    Returns ((n, P_2d, geometry_data, simulation_parameters,
+    arrhythmia_parameters), pacing_ms (None: the reference's default),
+    electrode_xyz)."""
+    if s1_s2 is None:
+        s1_s2 = C2_S1_S2_MS
+    ijk = synthetic.shell((25.0, 20.0, 18.0), 0.4, wall, 4, 5.0, seed)
+    s1 = np.where(ijk[:, 0] < ijk[:, 0].min() + 3)[0]
+    s2 = np.where((ijk[:, 0] < 0) & (ijk[:, 1] > 0))[0]
+    case = synthetic.make_case(ijk, 0.4, 1, 0.02, t_phys, s1, s2_ids=s2, flag=1, s1_t=0.0, s1_s2=float(s1_s2))
+    rng = np.random.default_rng(seed + 64)
+    return case, None, synthetic.electrodes_off_surface(ijk, 0.4, n_electrodes, rng, offset=2.0)

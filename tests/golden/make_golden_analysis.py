@@ -1,11 +1,13 @@
-"""Generate ``tests/golden/analysis_*.npz``: electrode LAT and conduction
-velocity computed by the reference's OWN, unmodified
-``utility/lat_map.py::compute_electrode_lat`` and
+"""Generate ``tests/golden/analysis_*.npz``: electrode LAT, conduction
+velocity and the LAT map interpolated onto voxels, computed by the reference's
+OWN, unmodified ``utility/lat_map.py::compute_electrode_lat``,
+``utility/lat_map.py::interpolate_lat`` and
 ``utility/conduction_velocity.py::compute``.
 
-Test infrastructure only.  Needs the reference checkout (``/root/reference``),
-which exists only where the fixtures are generated; the fixtures are committed
-and nothing at test time reads the reference.  ``lat_map.py`` imports
+Test infrastructure only.  Needs a checkout of the reference, named by the
+environment variable ``PHS_REFERENCE_DIR``; it exists only where the fixtures
+are generated, the fixtures are committed and nothing at test time reads the
+reference.  ``lat_map.py`` imports
 matplotlib, scipy's interpolators and the reference's ``common`` module for its
 plotting helpers; matplotlib and ``common`` are replaced by empty stub modules
 (the two functions used here touch neither).
@@ -15,7 +17,15 @@ per electrode, with activation times from a point source (3-D shell surface)
 or a plane wave (flat sheet, where every electrode has the same z and the
 plane fit is rank-deficient), plus small noise.
 
-Run:  python tests/golden/make_golden_analysis.py
+``analysis_interp.npz`` holds the interpolation cases (``interpolate_lat``
+of the reference on the electrode LAT of the cases above, with the electrodes
+moved off the lattice by up to 0.05 mm, plus a 4 x 4
+electrode grid 1 mm above a sheet, whose constant z is dropped and whose
+border voxels lie outside the electrode hull); each case is checked to have no
+voxel whose two nearest electrodes are at equal distance, so the nearest-
+electrode fallback has one answer.
+
+Run:  PHS_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden_analysis.py
 """
 import importlib.util
 import os
@@ -24,7 +34,7 @@ import types
 
 import numpy as np
 
-REF = os.environ.get("PHS_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("PHS_REFERENCE_DIR", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
@@ -77,8 +87,43 @@ def cases():
     return out
 
 
+def _check_no_nearest_ties(vox_r, el_r):
+    """No voxel outside the electrode hull (the ones the nearest-electrode
+    fallback fills) has two electrodes at (nearly) the same distance."""
+    from scipy.interpolate import LinearNDInterpolator
+    outside = np.isnan(LinearNDInterpolator(el_r, np.zeros(el_r.shape[0]))(vox_r))
+    vox_r = vox_r[outside]
+    d2 = ((vox_r[:, None, :] - el_r[None, :, :]) ** 2).sum(axis=2)
+    s = np.sort(d2, axis=1)
+    assert np.all(s[:, 1] - s[:, 0] > 1e-9 * np.maximum(s[:, 1], 1.0)), "nearest-electrode tie"
+
+
+def interp_cases(lat_of):
+    """(name, voxel, electrode_xyz) of the interpolation fixture."""
+    from pyheartsim_b200 import synthetic
+    out = []
+    jit = np.random.default_rng(5)
+    for name, vox, ids, _ in cases():
+        # electrodes at the chosen voxels, moved by up to 0.05 mm in the
+        # dimensions they span (a constant dimension stays constant), so that no
+        # voxel outside their hull is equidistant from two of them
+        el = vox[ids].copy()
+        span = np.ptp(el, axis=0) > 0
+        el[:, span] += jit.uniform(-0.05, 0.05, size=(el.shape[0], int(span.sum())))
+        out.append((name, vox, el, lat_of[name]))
+    i, j = np.meshgrid(np.arange(40), np.arange(30), indexing="ij")
+    vox = np.stack([i.ravel() * 0.4, j.ravel() * 0.4, np.zeros(i.size)], axis=1)
+    el = synthetic.electrodes_grid(40, 30, 0.4)
+    rng = np.random.default_rng(11)
+    out.append(("grid_above_sheet", vox, el, rng.integers(0, 60, size=el.shape[0])))
+    return out
+
+
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "utility")):
+        raise SystemExit("set PHS_REFERENCE_DIR to a checkout of the reference")
     lat_map, cv = _load()
+    lat_of = {}
     for name, vox, ids, egm in cases():
         lat = lat_map.compute_electrode_lat(egm)
         vec, mag, mean = cv.compute({"electrogram_unipolar": egm},
@@ -88,6 +133,18 @@ def main():
                             cv_mean=np.float64(mean))
         print(name, egm.shape, "lat range", int(np.min(lat)), int(np.max(lat)), "nan rows",
               int(np.isnan(mag).sum()), "mean", mean)
+        lat_of[name] = np.asarray(lat)
+    fx = {}
+    for k, (name, vox, el, lat) in enumerate(interp_cases(lat_of)):
+        active = np.ptp(el, axis=0) > 0
+        lin = np.asarray(lat_map.interpolate_lat(vox, el, lat), dtype=np.float64)
+        _check_no_nearest_ties(vox[:, active], el[:, active])
+        fx.update({f"{k}_voxel": vox, f"{k}_electrode": el, f"{k}_lat_electrode": np.asarray(lat),
+                   f"{k}_lat_voxel": lin})
+        print("interp", name, vox.shape[0], "voxels", el.shape[0], "electrodes, dims", int(active.sum()),
+              "outside the hull", int(np.isnan(lat_map.LinearNDInterpolator(el[:, active], lat)(vox[:, active])).sum()))
+    fx["names"] = np.array([c[0] for c in interp_cases(lat_of)])
+    np.savez_compressed(os.path.join(HERE, "analysis_interp.npz"), **fx)
 
 
 if __name__ == "__main__":

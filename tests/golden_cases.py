@@ -10,13 +10,24 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def names():
-    """Simulation fixtures (the analysis_* files hold electrode LAT / CV cases)."""
+    """Simulation fixtures of the reference's own runs (the analysis_* files hold
+    electrode LAT / CV / interpolation cases, c1_* the oracle's sheet run)."""
     return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(f).startswith("analysis_"))
+                  if not os.path.basename(f).startswith(("analysis_", "c1_")))
 
 
 def analysis_names():
-    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "analysis_*.npz")))
+    """The electrode LAT / conduction-velocity fixtures (not the interpolation one)."""
+    return sorted(os.path.basename(f)[:-4] for f in glob.glob(os.path.join(GOLDEN, "analysis_*.npz"))
+                  if not f.endswith("analysis_interp.npz"))
+
+
+def interp_cases():
+    """[(name, voxel, electrode_xyz, lat_electrode, lat_voxel)] of the reference's
+    own interpolate_lat (tests/golden/analysis_interp.npz)."""
+    g = np.load(os.path.join(GOLDEN, "analysis_interp.npz"), allow_pickle=False)
+    return [(str(nm), g[f"{k}_voxel"], g[f"{k}_electrode"], g[f"{k}_lat_electrode"], g[f"{k}_lat_voxel"])
+            for k, nm in enumerate(g["names"])]
 
 
 def load(name):

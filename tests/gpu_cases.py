@@ -19,16 +19,7 @@ def slab_ap(nx=16, ny=16, nz=4, t_phys=40.0, dt=0.1):
 
 
 def small_shell_ms(seed=1, t_phys=40.0, dt=0.05, scar_cov=0.15, fibres=False):
-    ijk = synthetic.shell((9.0, 8.0, 7.0), 0.4, 3, 2, 2.0, seed)
-    rng = np.random.default_rng(seed)
-    from pyheartsim_b200.geometry import lattice_neighbors
-    nb = lattice_neighbors(ijk)
-    c = synthetic.scar(ijk, nb, scar_cov, rng)
-    healthy = np.where(c == 1.0)[0]
-    centre = ijk[healthy[int(rng.integers(0, healthy.size))]]
-    s1 = np.where(np.sum((ijk - centre) ** 2, axis=1) <= 9)[0]
-    D0 = synthetic.fibre_tensors(ijk) if fibres else None
-    return synthetic.make_case(ijk, 0.4, 0, dt, t_phys, s1, flag=4, c_scale=c, D0=D0), 2.0
+    return synthetic.small_shell_case(seed, t_phys, dt, scar_cov, fibres)
 
 
 def small_shell_ms_fibres():

@@ -76,3 +76,30 @@ def test_result_file_from_the_device_history(tmp_path, cuda_device):
     np.testing.assert_array_equal(f["electrogram_unipolar"], egm)
     np.testing.assert_array_equal(f["lat_electrode"], lat)
     np.testing.assert_array_equal(f["physical_time"], t)
+
+
+INTERP_ATOL = 1e-12   # barycentric sums: the same operations as scipy, a different simplex on shared facets
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_interpolate_lat_matches_reference(k, cuda_device):
+    """utility/lat_map.py:29-46 on the device against the reference's own
+    interpolate_lat: 3-D shell, flat sheet (constant z dropped), sparse 3-D
+    points, and a 4 x 4 electrode grid above a sheet (nearest fallback on the
+    border)."""
+    name, vox, el, lat_e, lat_v = golden_cases.interp_cases()[k]
+    out = analysis.interpolate_lat(vox, el, lat_e)
+    assert out.dtype == np.float64 and out.shape == lat_v.shape
+    np.testing.assert_array_equal(np.isnan(out), np.isnan(lat_v))
+    np.testing.assert_allclose(out, lat_v, rtol=0, atol=INTERP_ATOL)
+
+
+def test_interpolate_lat_random_3d_matches_oracle(cuda_device):
+    rng = np.random.default_rng(21)
+    el = rng.uniform(0, 20, size=(300, 3))
+    vox = rng.uniform(-2, 22, size=(20000, 3))
+    lat = rng.uniform(0, 80, size=300)
+    out = analysis.interpolate_lat(vox, el, lat)
+    ref = oracle_analysis.interpolate_lat(vox, el, lat)
+    np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+    np.testing.assert_allclose(out, ref, rtol=0, atol=INTERP_ATOL)

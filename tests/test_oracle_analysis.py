@@ -18,3 +18,11 @@ def test_oracle_matches_reference_analysis(name):
     np.testing.assert_allclose(vec, g["cv_vectors"], rtol=1e-12, atol=0)
     np.testing.assert_allclose(mag, g["cv_magnitudes"], rtol=1e-12, atol=0)
     assert abs(mean - float(g["cv_mean"])) <= 1e-12 * abs(float(g["cv_mean"]))
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_oracle_interpolate_lat_matches_reference(k):
+    name, vox, el, lat_e, lat_v = golden_cases.interp_cases()[k]
+    out = analysis.interpolate_lat(vox, el, lat_e)
+    np.testing.assert_array_equal(np.isnan(out), np.isnan(lat_v))
+    np.testing.assert_array_equal(out, lat_v)          # same scipy routines: bit-exact

@@ -32,7 +32,9 @@ def test_noalloc_matches_allocating_entry_point_twice(cuda_device):
     import torch
     L = _lib.lib()
     stream = torch.cuda.current_stream().cuda_stream
-    shapes = [(300, 20000, 64), (123, 7777, 40)]   # two calls in a row, different sizes
+    # calls in a row, different sizes; the last fills the scratch exactly
+    # (T * n_e = 2^21), which leaves room for one split-K slice only
+    shapes = [(300, 20000, 64), (123, 7777, 40), (2048, 4096, 1024)]
     for call, (T, n_v, n_e) in enumerate(shapes):
         g = torch.Generator(device="cpu").manual_seed(100 + call)
         V = torch.randn(T, n_v, dtype=torch.float64, generator=g).to(cuda_device)
