@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--accuracy-only", action="store_true", help="run only the accuracy leg")
     p.add_argument("--no-tune", action="store_true", help="use the default step-kernel variant")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
-    p.add_argument("--serving-requests", type=int, default=16)
+    p.add_argument("--serving-requests", type=int, default=300)
     p.add_argument("--egm-nv", type=int, default=500_000)
     p.add_argument("--egm-ne", type=int, default=2048)
     p.add_argument("--egm-T", type=int, default=1000)
@@ -191,8 +191,13 @@ def run_b200(args):
     insts = [compile_case(c, m, args.tol) for c, m in cases]
     ns = np.array([m["n"] for _, m in cases], dtype=np.int64)
     S = max(1, args.steps_per_launch)
-    K = (args.steps + S - 1) // S * S
-    W = max(3, (args.warmup + S - 1) // S * S)
+    K = max(1, args.steps)
+    W = max(3, args.warmup)
+
+    def launches_of(count):
+        """Launch sizes covering exactly ``count`` steps: full launches of S
+        steps, then the remainder."""
+        return [S] * (count // S) + ([count % S] if count % S else [])
     stream = torch.cuda.current_stream(dev)
 
     eng = BatchedEngine(_lib.PREC_F32)
@@ -221,8 +226,8 @@ def run_b200(args):
             eng.advance(S, stream=stream, sync=False)
     eng.rebalance()
     eng.set_profile(False)
-    for _ in range(max(1, W // S)):
-        eng.advance(S, stream=stream, sync=False)
+    for k in launches_of(W):
+        eng.advance(k, stream=stream, sync=False)
     torch.cuda.synchronize(dev)
     info0 = [eng.info(s) for s in slots]
     launches0 = eng.launches()
@@ -239,8 +244,8 @@ def run_b200(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(K // S):
-        eng.advance(S, stream=stream, sync=False)
+    for k in launches_of(K):
+        eng.advance(k, stream=stream, sync=False)
     ev1.record(stream)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
@@ -307,11 +312,11 @@ def run_b200(args):
             line["anisotropic"] = aniso_leg(args, dev, tune, count=args.aniso_instances)
             line["geometry"] = geometry_leg(args, dev)
             del cases
-            line["serving"] = serving_leg(args, line["plain_fp64"]["value"], dev)
+            line["serving"] = serving_leg(args, dev, count=args.serving_requests)
             # latency below saturation: Poisson arrivals offering half the batched
-            # throughput, shorter requests (100-400 ms)
-            line["serving_half_load"] = serving_leg(args, line["plain_fp64"]["value"], dev, load=(0.5, value),
-                                                    dur_ms=(100.0, 400.0), count=12)
+            # throughput, same time compression
+            line["serving_half_load"] = serving_leg(args, dev, count=max(50, args.serving_requests // 3),
+                                                    load=(0.5, value), plain_subset=0)
             line["electrogram"] = egm_leg(args, dev)
             line["cpu_baseline"] = cpu_leg(args)
     if world > 1:
@@ -633,7 +638,7 @@ def accuracy_leg(dev, tol, walls=(3, 8), c3_count=4):
         case, pdur, el = workloads.atrium_c2(wall=w)
         r = accuracy.compare_case(case, pdur, el, tol=tol)
         r["wall_voxels"] = int(w)
-        r["s1_s2_ms"] = workloads.C2_S1_S2_MS
+        r["s1_mm"], r["s1_s2_ms"] = workloads.C2_PACING.get(w, workloads.C2_PACING[3])
         out[f"c2_wall{w}"] = r
     sizes = workloads.batch_sizes(64, 50_000, 400_000, 0)
     picks = []
@@ -657,43 +662,73 @@ def accuracy_leg(dev, tol, walls=(3, 8), c3_count=4):
     return out
 
 
-def serving_leg(args, plain_rate, dev, load=None, dur_ms=(200.0, 2000.0), count=None):
+def serving_leg(args, dev, count=300, compress=20.0, rate=20.0, dur_ms=(200.0, 2000.0), load=None,
+                plain_subset=4):
     """Continuous batching under Poisson arrivals (20k-1M voxels, random model
-    and pacing site): latency percentiles and served throughput.  Default: 20
-    requests/s of 200-2000 ms, about 10x what one B200 can serve (the overload
-    case).  ``load = (fraction, capacity)``: instead, the arrival rate whose
-    requests offer that fraction of ``capacity`` voxel-steps/s (the measured
-    batched throughput).  The plain-FP64-serial comparison is an estimate from
-    the measured plain rate ``plain_rate`` (running it for real would take
-    hours)."""
+    and pacing site), time-compressed: simulated durations divided by
+    ``compress`` and the arrival rate multiplied by it, so the offered load in
+    voxel-steps/s is that of ``rate`` requests/s of ``dur_ms`` (several times
+    what one B200 serves) while ``count`` requests finish in seconds.  Latency
+    runs from arrival to the request's whole 1 kHz Vm history on the host.
+    ``load = (fraction, capacity)``: instead, the arrival rate whose requests
+    offer that fraction of ``capacity`` voxel-steps/s.
+
+    The plain-FP64-serial comparison is measured on the first ``plain_subset``
+    requests: each run alone through the plain FP64 path (GMRES(50) full
+    cycles), one after another in arrival order, compile to history on the
+    host; their FIFO latencies are set beside the same requests' latencies in
+    the continuous-batching run."""
     import torch
-    from pyheartsim_b200 import serving
-    count = count or args.serving_requests
-    rate = 20.0
+    from pyheartsim_b200 import _lib, serving, workloads
+    from pyheartsim_b200.engine import BatchedEngine
+    d = (dur_ms[0] / compress, dur_ms[1] / compress)
+    r_eff = rate * compress
     if load is not None:
         frac, capacity = load
-        probe = serving.poisson_requests(count, rate_per_s=1.0, dur_ms=dur_ms, seed=args.seed)
+        probe = serving.poisson_requests(count, rate_per_s=1.0, dur_ms=d, seed=args.seed)
         # voxel-steps of a request: physical dt 0.05 ms (MS) or 0.02 ms (AP)
         work = np.mean([r.n_target * r.duration_ms / (0.05 if r.model == 0 else 0.02) for r in probe])
-        rate = frac * capacity / work
-    reqs = serving.poisson_requests(count, rate_per_s=rate, dur_ms=dur_ms, seed=args.seed)
+        r_eff = frac * capacity / work
+    reqs = serving.poisson_requests(count, rate_per_s=r_eff, dur_ms=d, seed=args.seed)
+    t_prep = time.perf_counter()
+    serving.prepare_payloads(reqs)               # the clients' geometry and parameters (before the clock)
+    t_prep = time.perf_counter() - t_prep
     free = torch.cuda.mem_get_info(dev)[0]
     srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
                          stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True)
     done, totals = srv.run(reqs)
     srv.close()
     out = serving.summarize(done, totals, reqs)
-    out["builder"] = "device (neighbour table, P_2d and operator tables on the GPU, one stream per builder thread)"
-    # FIFO single-server schedule of the same requests at the plain FP64 rate
-    t = 0.0
-    lat = []
-    for r in sorted(done, key=lambda r: r.arrival_s):
-        t = max(t, r.arrival_s) + r.inst.n_voxel * r.inst.n_steps / plain_rate
-        lat.append(t - r.arrival_s)
-    out["plain_fp64_serial_estimate"] = {"p50_latency_s": float(np.percentile(lat, 50)),
-                                         "p99_latency_s": float(np.percentile(lat, 99)), "makespan_s": t}
-    out["arrival_rate_per_s"] = rate
-    out["durations_ms"] = list(dur_ms)
+    out["builder"] = ("requests carry voxel coordinates, scar conductivities, pacing site and parameter dicts "
+                      f"(made before the clock, {t_prep:.1f} s); the server builds neighbour table, P_2d and "
+                      "operator tables on the GPU, one stream per builder thread")
+    out["arrival_rate_per_s"] = r_eff
+    out["durations_ms"] = list(d)
+    out["time_compression"] = compress
+    if plain_subset:
+        by_id = {r.rid: r for r in done}
+        sub = sorted(reqs, key=lambda r: r.arrival_s)[:plain_subset]
+        t = 0.0
+        rows = []
+        for r in sub:
+            i = 2 * (r.seed % 1000) + r.model
+            t0 = time.perf_counter()
+            inst, _, _ = workloads.shell_case(i, r.n_target, r.seed // 1000, t_phys=r.duration_ms, fast=False)
+            eng = BatchedEngine(_lib.PREC_F64)
+            slot = eng.add(inst)
+            while not eng.finished(slot):
+                eng.advance(1000)
+            eng.history(slot)
+            eng.close()
+            run_s = time.perf_counter() - t0
+            t = max(t, r.arrival_s) + run_s
+            rows.append({"rid": r.rid, "voxels": int(inst.n_voxel), "steps": int(inst.n_steps), "run_s": run_s,
+                         "plain_serial_latency_s": t - r.arrival_s,
+                         "batched_latency_s": by_id[r.rid].done_s - by_id[r.rid].arrival_s})
+        out["plain_fp64_serial_subset"] = {
+            "requests": rows, "measured": True,
+            "voxel_steps_per_s": float(sum(x["voxels"] * x["steps"] for x in rows)
+                                       / max(sum(x["run_s"] for x in rows), 1e-9))}
     return out
 
 
@@ -771,6 +806,7 @@ def egm_leg(args, dev, history=None):
         _lib.check(L.phs_egm_contract_bf16x3(T, n_e, Tp, Ep, Kp, p(vh), p(vl), p(mh), p(ml), p(out), p(work), sp),
                    "contract_bf16x3")
     ev[5].record(stream)
+    _lib.check(L.phs_egm_bf16x3_status(p(work), sp), "contract_bf16x3 status")
     torch.cuda.synchronize()
     ms_bf = ev[4].elapsed_time(ev[5]) / reps
     ms_f64 = ev[2].elapsed_time(ev[3])

@@ -159,11 +159,18 @@ int64_t phs_engine_launch_count(phs_engine* eng);
                                     the two after it first call phs_engine_rebalance, so team
                                     sizes follow the measured cost; then the timers go off
                                     again.  0: team sizes change only on explicit rebalance  */
+#define PHS_CFG_WAVE_INSTANCES 6 /* at most this many instances per launch wave (0, the default: as
+                                    many as the grid holds).  Each wave is one launch over the whole
+                                    grid for the same steps, one wave after another, so a wave's
+                                    instances have the L2 to themselves                             */
 int phs_engine_config(phs_engine* eng, int key, int64_t value);
 /* Compiled step-kernel variants of a precision: count, and per variant the
  * minimum CTAs per SM it was compiled for and its register count (arrays of at
  * least *count entries, may be NULL).                                           */
 int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, int32_t* max_regs);
+/* Voxels per thread of each step-kernel variant of a precision (a tile is 256 x
+ * that many consecutive voxels); vpt must hold `count` >= the variant count.   */
+int phs_step_variant_vpt(int precision, int32_t count, int32_t* vpt);
 /* Re-split the CTAs over the instances in proportion to their cost since the
  * last rebalance: the measured team time per step x team CTAs when the phase
  * timers (PHS_CFG_PROFILE) are on, else voxels x (1.6 + Arnoldi iterations per
@@ -210,11 +217,17 @@ int phs_split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, int 
  * FP32 accumulation in TMEM, split-K partials reduced in a fixed order.
  * Vhi/Vlo: [T_pad][K_pad] bf16; Mhi/Mlo: [n_e_pad][K_pad] bf16 (device).
  * T_pad % 128 == 0, n_e_pad % 128 == 0, K_pad % 64 == 0.  work: device scratch
- * of phs_egm_bf16x3_workspace() bytes.                                            */
+ * of phs_egm_bf16x3_workspace() bytes, whose first 4 bytes are an error word.
+ * Asynchronous on `stream` (no host synchronisation): a contraction whose
+ * bounded pipeline waits gave up leaves the error word non-zero; read it with
+ * phs_egm_bf16x3_status.                                                        */
 int64_t phs_egm_bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
 int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
                             const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi,
                             const uint16_t* Mlo, float* egm, void* work, void* stream);
+/* Synchronise `stream` and read the error word of the last contraction that used
+ * `work`: PHS_OK, or PHS_ERR_TIMEOUT when its pipeline waits gave up.          */
+int phs_egm_bf16x3_status(const void* work, void* stream);
 /* Allocation-free form of phs_egm_contract_f64 (no counterpart in the reference).
  * For callers that cannot allocate device memory when they contract: inside a
  * global-mode stream capture, under another allocator that owns the device

@@ -34,6 +34,7 @@ CFG_CTAS_PER_SM = 2
 CFG_PROFILE = 3
 CFG_TEST_TEAM_OVERCOUNT = 4
 CFG_AUTO_BALANCE = 5
+CFG_WAVE_INSTANCES = 6
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
                  "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas")
 
@@ -152,6 +153,7 @@ SIGNATURES = {
     "phs_engine_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "phs_engine_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64]),
     "phs_step_variants": (ctypes.c_int, [ctypes.c_int, c_int32_p, c_int32_p, c_int32_p]),
+    "phs_step_variant_vpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, c_int32_p]),
     "phs_instance_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "phs_engine_rebalance": (ctypes.c_int, [ctypes.c_void_p]),
     "phs_simulate": (ctypes.c_int, [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
@@ -168,6 +170,7 @@ SIGNATURES = {
     "phs_egm_contract_bf16x3": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                                ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_egm_bf16x3_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "phs_egm_contract_f64_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                                     ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),

@@ -1,13 +1,21 @@
 """Autotuner of the step kernel.
 
-Times every compiled step-kernel variant (register budget) at every feasible
+Times every compiled step-kernel variant (voxels per thread, i.e. the tile
+length of 256 x VPT voxels, and register budget) at every feasible
 CTAs-per-SM setting on the engine's live instances, keeps the fastest and
-leaves the engine configured with it.  Tuning advances the instances like any
-other call (the steps are real work).  Results are cached per GPU name and
-workload bucket (total voxels rounded to a power of two, instance count) for
-the lifetime of the process.
+leaves the engine configured with it.  Each option is timed ``repeats`` times
+(one launch of ``steps`` steps each, after a warm launch that also captures
+its graph) and ranked by the median.  Tuning advances the instances like any
+other call (the steps are real work).
+
+Results are cached per GPU name and workload bucket (precision, total voxels
+rounded to a power of two, instance count): in the process, and in a JSON file
+(``PHS_AUTOTUNE_CACHE``, default ``~/.cache/pyheartsim_b200/autotune.json``)
+so later processes on the same machine start from the same choice.
 """
+import json
 import math
+import os
 
 import torch
 
@@ -17,22 +25,53 @@ from .engine import step_variants
 _CACHE = {}
 
 
+def cache_path():
+    return os.environ.get("PHS_AUTOTUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "pyheartsim_b200",
+                                                                "autotune.json")
+
+
+def _load_file():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store_file(key, best):
+    path = cache_path()
+    try:
+        data = _load_file()
+        data[key] = list(best)
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + f".{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass                                   # a read-only home: the in-process cache still works
+
+
 def _bucket(engine):
     n = sum(engine.instance(s).n_voxel for s in engine.slots())
-    return (torch.cuda.get_device_name(), engine.precision, 1 << max(0, int(math.log2(max(n, 1)))),
-            len(engine.slots()))
+    return "|".join(str(x) for x in (torch.cuda.get_device_name(), engine.precision,
+                                      1 << max(0, int(math.log2(max(n, 1)))), len(engine.slots())))
 
 
-def tune(engine, steps=10, stream=None, cps_options=None):
+def tune(engine, steps=10, stream=None, cps_options=None, repeats=5, use_file=True):
     """Pick (variant, ctas_per_sm) for ``engine``; returns the timing table."""
     key = _bucket(engine)
+    if key not in _CACHE and use_file:
+        hit = _load_file().get(key)
+        if hit is not None:
+            _CACHE[key] = tuple(hit)
     if key in _CACHE:
         best = _CACHE[key]
         engine.configure(variant=best[0], ctas_per_sm=best[1])
         return {"cached": True, "best": best}
     stream = stream or torch.cuda.current_stream()
     table = []
-    for variant, minb, regs in step_variants(engine.precision):
+    for variant, minb, regs, vpt in step_variants(engine.precision, with_vpt=True):
         options = cps_options or sorted({minb, max(1, minb - 1), minb + 1})
         for cps in options:
             engine.configure(variant=variant, ctas_per_sm=cps)
@@ -40,15 +79,22 @@ def tune(engine, steps=10, stream=None, cps_options=None):
                 engine.advance(steps, stream=stream, sync=True)      # plan + graph capture, warm
             except _lib.PhsError:
                 continue
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            engine.advance(steps, stream=stream, sync=False)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            table.append({"variant": variant, "min_ctas": minb, "regs": regs, "ctas_per_sm": cps,
-                          "ms_per_step": e0.elapsed_time(e1) / steps})
+            times = []
+            for _ in range(max(1, repeats)):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                engine.advance(steps, stream=stream, sync=False)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1) / steps)
+            times.sort()
+            table.append({"variant": variant, "voxels_per_thread": vpt, "min_ctas": minb, "regs": regs,
+                          "ctas_per_sm": cps, "ms_per_step": times[len(times) // 2],
+                          "ms_per_step_min": times[0], "ms_per_step_max": times[-1]})
     best = min(table, key=lambda r: r["ms_per_step"])
     _CACHE[key] = (best["variant"], best["ctas_per_sm"])
+    if use_file:
+        _store_file(key, _CACHE[key])
     engine.configure(variant=best["variant"], ctas_per_sm=best["ctas_per_sm"])
     return {"cached": False, "best": (best["variant"], best["ctas_per_sm"]), "table": table}

@@ -227,6 +227,7 @@ int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int6
                     const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo,
                     float* egm, void* work, cudaStream_t stream);
 int64_t bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
+int bf16x3_status(const void* work, cudaStream_t stream);
 int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src_f64, uint16_t* hi,
                uint16_t* lo, int64_t rows_out, int64_t ld_out, cudaStream_t stream);
 
@@ -275,6 +276,8 @@ int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_p
                             float* egm, void* work, void* stream) {
     return contract_bf16x3(T, n_e, T_pad, n_e_pad, K_pad, Vhi, Vlo, Mhi, Mlo, egm, work, (cudaStream_t)stream);
 }
+
+int phs_egm_bf16x3_status(const void* work, void* stream) { return bf16x3_status(work, (cudaStream_t)stream); }
 
 int phs_electrogram(int64_t T, int64_t n_v, int64_t n_e, const double* V, const double* voxel_xyz,
                     const double* electrode_xyz, const double* c_voxel, const double* D0, const int32_t* in_ptr,
@@ -338,6 +341,7 @@ int phs_electrogram(int64_t T, int64_t n_v, int64_t n_e, const double* V, const 
         rc = split_bf16(T, n_v, dV, n_v, true, vh, vl, Tp, Kp, s);
         if (rc == PHS_OK) rc = split_bf16(n_e, n_v, dMt, n_v, true, mh, ml, Ep, Kp, s);
         if (rc == PHS_OK) rc = contract_bf16x3(T, n_e, Tp, Ep, Kp, vh, vl, mh, ml, e32, work, s);
+        if (rc == PHS_OK) rc = bf16x3_status(work, s);
         if (rc == PHS_OK) rc = normalize(T, n_e, e32, false, s);
         if (rc == PHS_OK) {
             const int64_t MN = T * n_e;

@@ -382,10 +382,18 @@ int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int64_
     int* err = (int*)work;
     float* part = (float*)((char*)work + kTcHeader);
     PHS_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
-    static bool attr_set = false;
-    if (!attr_set) {
-        PHS_CUDA_TRY(cudaFuncSetAttribute(egm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-        attr_set = true;
+    // the dynamic shared-memory opt-in is a per-device attribute of the kernel
+    {
+        static std::mutex mu;
+        static bool attr_set[64] = {};
+        int dev = 0;
+        PHS_CUDA_TRY(cudaGetDevice(&dev));
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+            PHS_CUDA_TRY(cudaFuncSetAttribute(egm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)TC_SMEM));
+            if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        }
     }
     dim3 grid((unsigned)(T_pad / TC_BM), (unsigned)(E_pad / TC_BN), (unsigned)splits);
     egm_bf16x3_kernel<<<grid, TC_THREADS, TC_SMEM, stream>>>(mv_hi, mv_lo, mm_hi, mm_lo, (int)(K_pad / TC_BK), per,
@@ -395,9 +403,16 @@ int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int64_
     tc_reduce_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 8192), 256, 0, stream>>>(
         T, n_e, T_pad, E_pad, splits, part, egm);
     PHS_CUDA_TRY(cudaGetLastError());
+    return PHS_OK;
+}
+
+// Error word of the last contraction that used `work`, read after `stream`
+// has finished it (synchronises the stream).
+int bf16x3_status(const void* work, cudaStream_t stream) {
+    if (!work) return PHS_ERR_BAD_ARG;
     PHS_CUDA_TRY(cudaStreamSynchronize(stream));
     int herr = 0;
-    PHS_CUDA_TRY(cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost));
+    PHS_CUDA_TRY(cudaMemcpy(&herr, work, sizeof(int), cudaMemcpyDeviceToHost));
     return herr ? PHS_ERR_TIMEOUT : PHS_OK;
 }
 

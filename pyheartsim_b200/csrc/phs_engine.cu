@@ -707,15 +707,6 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     // ---- sample / activation bookkeeping of the state in u (after step s-1)
-    // the same with the activation entry already loaded (lat_n; read only when
-    // un >= 0.5 after a completed step)
-    auto sample_loaded = [&](long long n, T un, T hn, int32_t lat_n, long long done_step) {
-        if (pending >= 0) {
-            I.hist_u[(size_t)pending * N + n] = un;
-            if (I.save_h) I.hist_h[(size_t)pending * N + n] = hn;
-        }
-        if (done_step >= 0 && un >= T(0.5) && lat_n < 0) I.lat[n] = (int32_t)done_step;
-    };
     auto sample_voxel = [&](long long n, T un, T hn, long long done_step) {
         if (pending >= 0) {
             I.hist_u[(size_t)pending * N + n] = un;
@@ -724,9 +715,32 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         if (done_step >= 0 && un >= T(0.5) && I.lat[n] < 0) I.lat[n] = (int32_t)done_step;
     };
 
-    // acc[v] += sum_{i < cnt} coef[i] * Vb[i][n_v], loads issued kChunk vectors at a time
     T* Vb = I.V;
     const size_t ldV = (size_t)N;
+
+    // End-of-step work of voxel n whose new state un is known (the state after
+    // step done_step): its sample into history slot `slot` (-1: none), its
+    // activation entry (lat_n loaded when un >= 0.5), then the RK4 reaction of
+    // the next step (stimulus bits stim_next) -> h of the step after it into
+    // hdst, u* into the basis column 1.  This is the reaction pass of the next
+    // step, done while the voxel's new state is still in registers.
+    auto react_voxel = [&](long long n, T un, T hn, int32_t lat_n, long long done_step, int slot, uint8_t fl,
+                           uint8_t stim_next, T* hdst) {
+        if (slot >= 0) {
+            I.hist_u[(size_t)slot * N + n] = un;
+            if (I.save_h) I.hist_h[(size_t)slot * N + n] = hn;
+        }
+        if (done_step >= 0 && un >= T(0.5) && lat_n < 0) I.lat[n] = (int32_t)done_step;
+        T p[5];
+        params_of(n, p);
+        const T J = (fl & stim_next & 3u) ? I.jmag : T(0);
+        T us, hs;
+        rk4(I.model, un, hn, J, p, I.dt, us, hs);
+        hdst[n] = hs;
+        Vb[(size_t)N + n] = us;
+    };
+
+    // acc[v] += sum_{i < cnt} coef[i] * Vb[i][n_v], loads issued kChunk vectors at a time
     auto axpy_basis = [&](int tile, int cnt, const double* coef, double (&acc)[VPT]) {
         for (int i0 = 0; i0 < cnt; i0 += kChunk) {
             T vv[kChunk][VPT];
@@ -748,21 +762,27 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
     };
 
+    // the reaction pass of the current step was done at the end of the previous
+    // one (by the same threads, for the same voxels)
+    bool prepared = false;
     for (; step < step_end && !retired && !aborted; ++step) {
         const uint8_t stim_bits = __ldg(I.stim + step);
         const bool tb = step < I.tb_steps;
-        const T* hin = hbuf ? I.h1 : I.h0;
+        T* hin = hbuf ? I.h1 : I.h0;
         T* hout = hbuf ? I.h0 : I.h1;
 
         // ================= RHS phase.  Pass 1: RK4 reaction of every voxel of the
         // team; u* goes to basis column 1 (unused until the first Arnoldi step).
+        // Except in the first step of a launch and after a full-cycle solve, it
+        // ran at the end of the previous step (react_voxel in the update and copy
+        // passes), so it costs no pass of its own.
         // Pass 2, after a team barrier: b = u* + dt/2 L u*, the initial guess and
         // r0 = b - A x0 -> V0, gathering u* of the neighbours from memory.  (A
         // fused form that kept a tile's u* in shared memory and recomputed the RK4
         // of neighbours outside the tile did three RK4 per voxel in row order and
         // was 17 % slower over the batch.)
         T* Us = Vb + ldV;
-        for (int tile = rank; tile < I.n_tiles; tile += P) {
+        for (int tile = prepared ? I.n_tiles : rank; tile < I.n_tiles; tile += P) {
             if (threadIdx.x < 4) {
                 const int t = threadIdx.x;
                 if (t == 0) pf_slice(I.u, sizeof(T), tile + P);
@@ -796,16 +816,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 #pragma unroll
             for (int v = 0; v < VPT; ++v) {
                 const long long n = voxel(tile, v);
-                if (n < N) {
-                    sample_loaded(n, un[v], hn[v], lt[v], step - 1);
-                    T p[5];
-                    params_of(n, p);
-                    const T J = (fl[v] & stim_bits & 3u) ? I.jmag : T(0);
-                    T us, hs;
-                    rk4(I.model, un[v], hn[v], J, p, I.dt, us, hs);
-                    hout[n] = hs;
-                    Us[n] = us;
-                }
+                if (n < N) react_voxel(n, un[v], hn[v], lt[v], step - 1, pending, fl[v], stim_bits, hout);
             }
         }
         pending = -1;
@@ -862,6 +873,14 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         if (!team_sync(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
         int act = read_action();
         mark(PF_RHS_WAIT);
+        // end of this step: its history slot, and whether the pass that writes
+        // the new state also runs the next step's reaction (not after the last
+        // step of the launch)
+        const bool due_now = (I.stride > 0) ? (step % I.stride == 0) : true;
+        const int slot_now = (due_now && id_save < I.n_samples) ? id_save : -1;
+        const bool fuse_next = step + 1 < step_end;
+        const uint8_t stim_next = fuse_next ? __ldg(I.stim + step + 1) : (uint8_t)0;
+        bool fused = false;
 
         if (act == ACT_CYCLE) {
             bool leave_solve = false;
@@ -977,16 +996,23 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 const int k = ctl.k;
                 load_shc(k);
                 const bool final = (act == ACT_UPDATE_FINAL);
+                const bool react = final && fuse_next;
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
                     if (threadIdx.x < k) pf_slice(Vb + (size_t)threadIdx.x * ldV, sizeof(T), tile + P);
                     else if (threadIdx.x == k) pf_slice(I.x, sizeof(T), tile + P);
                     else if (threadIdx.x == k + 1 && final) pf_slice(I.dx, sizeof(T), tile + P);
+                    else if (threadIdx.x == k + 2 && react) pf_slice(hout, sizeof(T), tile + P);
+                    else if (threadIdx.x == k + 3 && react) pf_slice(I.vflags, 1, tile + P);
                     double acc[VPT], x_in[VPT];
+                    T hn[VPT];
+                    uint8_t fl[VPT];
 #pragma unroll
                     for (int v = 0; v < VPT; ++v) {
                         const long long n = voxel(tile, v);
                         acc[v] = (n < N) ? (double)I.x[n] : 0.0;
                         x_in[v] = acc[v];
+                        hn[v] = (react && n < N) ? hout[n] : T(0);
+                        fl[v] = (react && n < N) ? __ldg(I.vflags + n) : (uint8_t)0;
                     }
                     axpy_basis(tile, k, shc, acc);
 #pragma unroll
@@ -1002,9 +1028,25 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             }
                         }
                     }
+                    if (react) {
+                        int32_t lt[VPT];
+#pragma unroll
+                        for (int v = 0; v < VPT; ++v) {
+                            const long long n = voxel(tile, v);
+                            lt[v] = (n < N && (T)acc[v] >= T(0.5)) ? I.lat[n] : 0;
+                        }
+#pragma unroll
+                        for (int v = 0; v < VPT; ++v) {
+                            const long long n = voxel(tile, v);
+                            if (n < N) react_voxel(n, (T)acc[v], hn[v], lt[v], step, slot_now, fl[v], stim_next, hin);
+                        }
+                    }
                 }
                 mark(PF_X);
-                if (final) break;
+                if (final) {
+                    fused = react;
+                    break;
+                }
                 // ============ true residual of the new iterate (start of the next cycle)
                 if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
@@ -1048,18 +1090,37 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             const T* src = (act == ACT_ZERO_B) ? I.b : I.x;
             for (int tile = rank; tile < I.n_tiles; tile += P) {
                 if (threadIdx.x == 0) pf_slice(src, sizeof(T), tile + P);
-                T cv[VPT];
+                else if (threadIdx.x == 1 && fuse_next) pf_slice(hout, sizeof(T), tile + P);
+                else if (threadIdx.x == 2 && fuse_next) pf_slice(I.vflags, 1, tile + P);
+                T cv[VPT], hn[VPT];
+                uint8_t fl[VPT];
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
                     const long long n = voxel(tile, v);
                     cv[v] = (n < N) ? src[n] : T(0);
+                    hn[v] = (fuse_next && n < N) ? hout[n] : T(0);
+                    fl[v] = (fuse_next && n < N) ? __ldg(I.vflags + n) : (uint8_t)0;
                 }
 #pragma unroll
                 for (int v = 0; v < VPT; ++v) {
                     const long long n = voxel(tile, v);
                     if (n < N) I.u[n] = cv[v];
                 }
+                if (fuse_next) {
+                    int32_t lt[VPT];
+#pragma unroll
+                    for (int v = 0; v < VPT; ++v) {
+                        const long long n = voxel(tile, v);
+                        lt[v] = (n < N && cv[v] >= T(0.5)) ? I.lat[n] : 0;
+                    }
+#pragma unroll
+                    for (int v = 0; v < VPT; ++v) {
+                        const long long n = voxel(tile, v);
+                        if (n < N) react_voxel(n, cv[v], hn[v], lt[v], step, slot_now, fl[v], stim_next, hin);
+                    }
+                }
             }
+            fused = fuse_next;
         } else {  // ACT_FAIL
             retired = true;
             break;
@@ -1070,8 +1131,11 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         // of the next step follows its mid-RHS barrier.
         if (prof_on && threadIdx.x == 0) pf[PF_STEPS] += 1;
         hbuf ^= 1;
-        const bool due = (I.stride > 0) ? (step % I.stride == 0) : true;
-        if (due && id_save < I.n_samples) pending = id_save++;
+        if (slot_now >= 0) {
+            ++id_save;
+            pending = fused ? -1 : slot_now;    // a fused pass wrote the sample already
+        }
+        prepared = fused;
     }
 
     // flush the sample and activation test of the last completed step
@@ -1232,6 +1296,7 @@ struct phs_engine {
     bool profile = false;    // per-instance phase timers
     bool test_overcount = false;  // test hook: first team waits for one CTA too many
     int default_cps = 0;     // CTAs per SM when advance() is given 0 (0: occupancy limit)
+    int wave_instances = 0;  // instances per launch wave (0: as many as the grid holds)
 };
 
 namespace {
@@ -1602,11 +1667,14 @@ int build_plan(phs_engine* e, int cps, bool edge) {
     }
     PHS_CUDA_TRY(cudaMemcpy(e->d_desc, descs.data(), bytes, cudaMemcpyHostToDevice));
 
-    // waves of at most G instances
+    // waves of at most G instances (fewer with wave_instances: each wave is a
+    // launch of its own over the whole grid, so the instances of a wave share
+    // the L2 with fewer others)
     std::vector<int4> map_all;
     std::vector<std::pair<size_t, int>>& waves = e->waves;  // (offset into map, grid)
-    for (size_t w0 = 0; w0 < act.size(); w0 += (size_t)G) {
-        size_t w1 = std::min(act.size(), w0 + (size_t)G);
+    const size_t per_wave = (size_t)((e->wave_instances > 0) ? std::min(G, e->wave_instances) : G);
+    for (size_t w0 = 0; w0 < act.size(); w0 += per_wave) {
+        size_t w1 = std::min(act.size(), w0 + per_wave);
         std::vector<int> tiles;
         std::vector<double> weight;
         bool measured = true;
@@ -1910,6 +1978,34 @@ int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, i
     return PHS_OK;
 }
 
+namespace {
+// Phase timers on or off for every instance (counters reset).
+int set_profile(phs_engine* e, bool on) {
+    cudaDeviceSynchronize();
+    e->profile = on;
+    for (auto& h : e->inst) {
+        if (!h.used) continue;
+        if (e->profile && !h.prof) {
+            if (cudaMalloc((void**)&h.prof, kProfSlots * sizeof(unsigned long long)) != cudaSuccess)
+                return PHS_ERR_OOM;
+        }
+        if (h.prof) cudaMemset(h.prof, 0, kProfSlots * sizeof(unsigned long long));
+        if (!e->profile && h.prof) { cudaFree(h.prof); h.prof = nullptr; }
+        for (int i = 0; i < kProfSlots; ++i) h.prof_ref[i] = 0;
+    }
+    e->dirty = true;
+    return PHS_OK;
+}
+}  // namespace
+
+int phs_step_variant_vpt(int precision, int32_t count, int32_t* vpt) {
+    if (precision != PHS_PREC_F32 && precision != PHS_PREC_F64) return PHS_ERR_BAD_ARG;
+    const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
+    if (count < nv || !vpt) return PHS_ERR_BAD_ARG;
+    for (int v = 0; v < nv; ++v) vpt[v] = precision == PHS_PREC_F64 ? kVptF64 : kVptF32;
+    return PHS_OK;
+}
+
 int phs_engine_config(phs_engine* e, int key, int64_t value) {
     if (!e) return PHS_ERR_BAD_ARG;
     switch (key) {
@@ -1934,19 +2030,15 @@ int phs_engine_config(phs_engine* e, int key, int64_t value) {
             e->dirty = true;
             return PHS_OK;
         case PHS_CFG_PROFILE:
-            cudaDeviceSynchronize();
-            e->profile = value != 0;
-            for (auto& h : e->inst) {
-                if (!h.used) continue;
-                if (e->profile && !h.prof) {
-                    if (cudaMalloc((void**)&h.prof, kProfSlots * sizeof(unsigned long long)) != cudaSuccess)
-                        return PHS_ERR_OOM;
-                }
-                if (h.prof) cudaMemset(h.prof, 0, kProfSlots * sizeof(unsigned long long));
-                if (!e->profile && h.prof) { cudaFree(h.prof); h.prof = nullptr; }
-                for (int i = 0; i < kProfSlots; ++i) h.prof_ref[i] = 0;
+            // the caller's setting wins over the automatic balancing's
+            e->auto_prof = false;
+            return set_profile(e, value != 0);
+        case PHS_CFG_WAVE_INSTANCES:
+            if (value < 0 || value > (1 << 20)) return PHS_ERR_BAD_ARG;
+            if (e->wave_instances != (int)value) {
+                e->wave_instances = (int)value;
+                e->dirty = true;
             }
-            e->dirty = true;
             return PHS_OK;
         default:
             return PHS_ERR_BAD_ARG;

@@ -128,10 +128,14 @@ class BatchedEngine:
     def config(self, key, value):
         _lib.check(_lib.lib().phs_engine_config(self._h, int(key), int(value)), "phs_engine_config")
 
-    def configure(self, variant=None, ctas_per_sm=None, auto_balance=None):
+    def configure(self, variant=None, ctas_per_sm=None, auto_balance=None, wave_instances=None):
         """Select the step-kernel variant and the CTAs per SM used by advance(),
-        and whether the 2nd and 3rd advance after an add/remove rebalance first."""
+        whether the 2nd and 3rd advance after an add/remove rebalance first, and
+        the most instances per launch wave (0: all in one wave)."""
         L = _lib.lib()
+        if wave_instances is not None:
+            _lib.check(L.phs_engine_config(self._h, _lib.CFG_WAVE_INSTANCES, int(wave_instances)),
+                       "phs_engine_config")
         if auto_balance is not None:
             _lib.check(L.phs_engine_config(self._h, _lib.CFG_AUTO_BALANCE, int(bool(auto_balance))),
                        "phs_engine_config")
@@ -178,12 +182,19 @@ class BatchedEngine:
             pass
 
 
-def step_variants(precision=_lib.PREC_F32):
-    """[(variant, min CTAs/SM it was compiled for, registers per thread)]."""
+def step_variants(precision=_lib.PREC_F32, with_vpt=False):
+    """[(variant, min CTAs/SM it was compiled for, registers per thread)], with
+    the voxels per thread (tile = 256 x VPT voxels) as a fourth entry when
+    ``with_vpt``."""
     n = ctypes.c_int32(0)
     _lib.check(_lib.lib().phs_step_variants(precision, ctypes.byref(n), None, None), "phs_step_variants")
     minb = np.zeros(n.value, dtype=np.int32)
     regs = np.zeros(n.value, dtype=np.int32)
     _lib.check(_lib.lib().phs_step_variants(precision, ctypes.byref(n), _lib.ptr(minb, ctypes.c_int32),
                                             _lib.ptr(regs, ctypes.c_int32)), "phs_step_variants")
+    if with_vpt:
+        vpt = np.zeros(n.value, dtype=np.int32)
+        _lib.check(_lib.lib().phs_step_variant_vpt(precision, n.value, _lib.ptr(vpt, ctypes.c_int32)),
+                   "phs_step_variant_vpt")
+        return [(i, int(minb[i]), int(regs[i]), int(vpt[i])) for i in range(n.value)]
     return [(i, int(minb[i]), int(regs[i])) for i in range(n.value)]

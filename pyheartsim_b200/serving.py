@@ -48,6 +48,7 @@ class Request:
         self.history = None
         self.history_bytes = 0
         self.status = None
+        self.payload = None        # the request's geometry and parameters (prepare_payloads)
 
 
 def poisson_requests(count, rate_per_s=20.0, n_min=20_000, n_max=1_000_000, dur_ms=(200.0, 2000.0), seed=0):
@@ -61,14 +62,45 @@ def poisson_requests(count, rate_per_s=20.0, n_min=20_000, n_max=1_000_000, dur_
     return [Request(i, float(t[i]), n[i], d[i], m[i], seed * 100_003 + i) for i in range(count)]
 
 
+def _payload_one(args):
+    i, n_target, seed, t_phys = args
+    return workloads.shell_payload(i, n_target, seed, t_phys=t_phys)
+
+
+def prepare_payloads(reqs, workers=None):
+    """Attach to each request what a client sends: its voxel coordinates, scar
+    conductivities, pacing site and parameter dicts (seeded synthetic shells,
+    made in a process pool; no tables).  The server's builder then only runs
+    the device compilation."""
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+    jobs = [(2 * (r.seed % 1000) + r.model, r.n_target, r.seed // 1000, r.duration_ms) for r in reqs]
+    workers = workers or min(len(jobs), max(1, (os.cpu_count() or 2) - 1), 32)
+    if workers <= 1:
+        out = [_payload_one(j) for j in jobs]
+    else:
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            out = list(ex.map(_payload_one, jobs, chunksize=4))
+    for r, p in zip(reqs, out):
+        r.payload = p
+
+
 _tls = threading.local()
 
 
 def build(req, tol=1e-7, restart=20, device=False):
     """Compile a request into an FP32 early-exit instance (shell geometry with
     scar).  ``device``: neighbour table, P_2d and operator tables on the GPU,
-    on a stream of the calling builder thread (same instance as the host path)."""
+    on a stream of the calling builder thread (same instance as the host path);
+    from the request's payload when it carries one."""
     i = 2 * (req.seed % 1000) + req.model        # parity of i selects the model in shell_case
+    if device and req.payload is not None:
+        import torch
+        if getattr(_tls, "stream", None) is None:
+            _tls.stream = torch.cuda.Stream()
+        with torch.cuda.stream(_tls.stream):
+            return workloads.compile_payload(req.payload, tol=tol, restart=restart, stream=_tls.stream)
     if device:
         import torch
         if getattr(_tls, "stream", None) is None:

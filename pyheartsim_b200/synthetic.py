@@ -80,7 +80,9 @@ def shell_for_size(n_target, seed=0, Delta=0.4, wall=3, base=(25.0, 20.0, 18.0),
 def scar(ijk, nb, coverage, rng, c_border=0.1, n_blobs=6, width=8.0):
     """Conductivity scale (n,): Gaussian-blob field thresholded to ``coverage``;
     0 inside, ``c_border`` on the one-voxel ring around the scar (face
-    neighbours ``nb[:, :6]``), 1 elsewhere."""
+    neighbours ``nb[:, :6]``; with ``nb`` None, the face neighbours are looked
+    up in a dense occupancy grid of the lattice coordinates, same result), 1
+    elsewhere."""
     n = ijk.shape[0]
     c = np.ones(n)
     if coverage <= 0:
@@ -91,12 +93,21 @@ def scar(ijk, nb, coverage, rng, c_border=0.1, n_blobs=6, width=8.0):
         f += np.exp(-np.sum((ijk - cc) ** 2, axis=1) / (2 * width ** 2))
     thr = np.quantile(f, 1.0 - coverage)
     core = f >= thr
-    nbs = nb[:, :6]
     ring = np.zeros(n, dtype=bool)
-    for k in range(6):
-        q = nbs[:, k]
-        ok = q >= 0
-        ring[ok] |= core[q[ok]]
+    if nb is None:
+        lo = ijk.min(axis=0) - 1
+        g = ijk - lo
+        grid = np.zeros(tuple(g.max(axis=0) + 2), dtype=bool)
+        grid[g[core, 0], g[core, 1], g[core, 2]] = True
+        for d in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            q = g + np.asarray(d)
+            ring |= grid[q[:, 0], q[:, 1], q[:, 2]]
+    else:
+        nbs = nb[:, :6]
+        for k in range(6):
+            q = nbs[:, k]
+            ok = q >= 0
+            ring[ok] |= core[q[ok]]
     ring &= ~core
     c[core] = 0.0
     c[ring] = c_border

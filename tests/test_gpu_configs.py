@@ -44,14 +44,18 @@ def test_c1_sheet_full_run_matches_oracle(cuda_device):
     assert rel < EGM_RTOL, rel
 
 
-def _fast_vs_plain(case, pdur, t_check):
+def _fast_vs_plain(case, pdur):
     n, P, geom, sp, ap = case
-    u64, _, _, lat64 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur,
-                                              return_lat=True)
+    u64, _, _, lat64, info = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur,
+                                                    return_lat=True, return_info=True)
     u32, _, _, lat32 = simulation_gpu.compute(n, P, geom, dict(sp), dict(ap), pacing_duration=pdur,
                                               dtype=np.float32, fast=True, tol=1e-7, return_lat=True)
-    assert np.array_equal(lat64 >= 0, lat32 >= 0), "a voxel activated in one precision only"
-    both = lat64 >= 0
+    # a voxel may cross Vm = 0.5 in one run's last step and one step after the
+    # end in the other; any other voxel activates in both runs or in neither
+    one = (lat64 >= 0) != (lat32 >= 0)
+    last = info["steps"] - FAST_LAT_STEPS
+    assert np.all(np.maximum(lat64[one], lat32[one]) >= last), "a voxel activated in one precision only"
+    both = (lat64 >= 0) & (lat32 >= 0)
     assert both.sum() > n // 20, "the case must propagate"
     dlat = int(np.abs(lat64[both].astype(np.int64) - lat32[both]).max())
     dvm = float(np.abs(u64 - u32).max())
@@ -62,7 +66,7 @@ def _fast_vs_plain(case, pdur, t_check):
 def test_c2_rotor_shell_full_geometry_first_40ms(cuda_device):
     (n, P, geom, sp, ap), pdur, _ = workloads.atrium_c2(wall=3, t_phys=40.0)
     assert n == 91292
-    _fast_vs_plain((n, P, geom, sp, ap), pdur, 40.0)
+    _fast_vs_plain((n, P, geom, sp, ap), pdur)
 
 
 @pytest.mark.parametrize("i", [0, 1])
@@ -72,4 +76,4 @@ def test_c3_batch_instances_first_40ms(i, cuda_device):
     sizes = workloads.batch_sizes(64, 50_000, 400_000, 0)
     _, case, meta = workloads.shell_case(i, int(sizes[i]), 0, t_phys=40.0)
     assert meta["model"] == i % 2
-    _fast_vs_plain(case, meta["pacing_ms"] / case[3]["time_scale"], 40.0)
+    _fast_vs_plain(case, meta["pacing_ms"] / case[3]["time_scale"])

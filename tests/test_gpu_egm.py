@@ -111,6 +111,7 @@ def test_bf16x3_contraction_device_pointers(T, K, E, cuda_device):
     out = torch.empty(T, E, dtype=torch.float32, device=cuda_device)
     _lib.check(L.phs_egm_contract_bf16x3(T, E, Tp, Ep, Kp, p(hA), p(lA), p(hB), p(lB), p(out), p(work), s),
                "contract")
+    _lib.check(L.phs_egm_bf16x3_status(p(work), s), "contract status")
     torch.cuda.synchronize()
     got = out.cpu().numpy().astype(np.float64)
     assert rel_l2(got, ref) < 1e-4
