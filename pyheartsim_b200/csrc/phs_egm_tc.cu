@@ -8,13 +8,18 @@
 // simulation/unipolar_electrogram_gpu.py:21-69 by a dense contraction of the
 // lead field (see phs_egm.cu) against the Vm history.
 //
-// One CTA computes a 128 (t) x 128 (e) tile over one K range (split-K):
-//   warp 0 lane 0   TMA producer: four 128x64 BF16 tiles per stage (Vhi, Vlo, Mhi,
-//                   Mlo), 128-byte swizzle, 3-stage mbarrier ring
+// One CTA computes a 128 (t) x 256 (e) tile over one K range (split-K):
+//   warp 0 lane 0   TMA producer: per stage two 128x64 BF16 tiles of V (hi, lo)
+//                   and two 256x64 tiles of M (hi, lo), 128-byte swizzle,
+//                   2-stage mbarrier ring (96 KB per stage)
 //   warp 1 lane 0   MMA issuer: per 64-wide K block, 4 K-slices x 3 products of
-//                   tcgen05.mma.cta_group::1.kind::f16 (M=128, N=128, K=16) into
-//                   one FP32 accumulator in TMEM; tcgen05.commit frees the stage
+//                   tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16) into
+//                   one FP32 accumulator in TMEM (256 columns); tcgen05.commit
+//                   frees the stage
 //   warps 0..3      epilogue: tcgen05.ld 32x32b.x32 -> FP32 partial tile in HBM
+// The 256-wide tile reads 96 KB of operands per 2 x 128 x 256 x 64 x 3 FLOPs,
+// 0.75 of what two 128 x 128 tiles read: the contraction streams its operands
+// from L2, so fewer bytes per FLOP keep the tensor pipe busier.
 // Split-K partials are summed in split order by a second kernel.
 //
 // Every wait is bounded (kTcWaitNs); on timeout the CTA records an error word,
@@ -33,13 +38,14 @@
 namespace phs {
 
 constexpr int TC_BM = 128;
-constexpr int TC_BN = 128;
+constexpr int TC_BN = 256;
 constexpr int TC_BK = 64;                       // 64 bf16 = 128 B rows (one swizzle atom)
-constexpr int TC_STAGES = 3;
-constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;  // 16 KB (TC_BM == TC_BN)
-constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;
+constexpr int TC_STAGES = 2;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;   // 16 KB
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;   // 32 KB
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_THREADS = 128;
-constexpr int TC_TMEM_COLS = 128;
+constexpr int TC_TMEM_COLS = TC_BN;
 constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 constexpr unsigned long long kTcWaitNs = 2000000000ull;  // 2 s
 constexpr int64_t kTcHeader = 256;                        // error word at the workspace head
@@ -140,7 +146,7 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)
 __global__ void __launch_bounds__(TC_THREADS, 1)
 egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_constant__ CUtensorMap map_vlo,
                   const __grid_constant__ CUtensorMap map_mhi, const __grid_constant__ CUtensorMap map_mlo,
-                  int nkb_total, int kb_per_split, int T_pad, int E_pad, float* __restrict__ part,
+                  int nkb_total, int kb_per_split, int T_pad, int part_cols, float* __restrict__ part,
                   int* __restrict__ err) {
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
@@ -189,10 +195,10 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
             uint8_t* st = smem + (size_t)s * TC_STAGE_BYTES;
             mbar_expect_tx(fb, TC_STAGE_BYTES);
             const int kc = (kb0 + i) * TC_BK;
-            tma_load_2d(smem_u32(st + 0 * TC_TILE_BYTES), &map_vhi, fb, kc, t0);
-            tma_load_2d(smem_u32(st + 1 * TC_TILE_BYTES), &map_vlo, fb, kc, t0);
-            tma_load_2d(smem_u32(st + 2 * TC_TILE_BYTES), &map_mhi, fb, kc, e0);
-            tma_load_2d(smem_u32(st + 3 * TC_TILE_BYTES), &map_mlo, fb, kc, e0);
+            tma_load_2d(smem_u32(st), &map_vhi, fb, kc, t0);
+            tma_load_2d(smem_u32(st + TC_A_BYTES), &map_vlo, fb, kc, t0);
+            tma_load_2d(smem_u32(st + 2 * TC_A_BYTES), &map_mhi, fb, kc, e0);
+            tma_load_2d(smem_u32(st + 2 * TC_A_BYTES + TC_B_BYTES), &map_mlo, fb, kc, e0);
             issued = i + 1;
         }
         // drain: every stage that was armed must have landed before the CTA leaves
@@ -212,10 +218,10 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint8_t* st = smem + (size_t)s * TC_STAGE_BYTES;
-            const uint64_t dAh = umma_desc_sw128(smem_u32(st + 0 * TC_TILE_BYTES));
-            const uint64_t dAl = umma_desc_sw128(smem_u32(st + 1 * TC_TILE_BYTES));
-            const uint64_t dBh = umma_desc_sw128(smem_u32(st + 2 * TC_TILE_BYTES));
-            const uint64_t dBl = umma_desc_sw128(smem_u32(st + 3 * TC_TILE_BYTES));
+            const uint64_t dAh = umma_desc_sw128(smem_u32(st));
+            const uint64_t dAl = umma_desc_sw128(smem_u32(st + TC_A_BYTES));
+            const uint64_t dBh = umma_desc_sw128(smem_u32(st + 2 * TC_A_BYTES));
+            const uint64_t dBl = umma_desc_sw128(smem_u32(st + 2 * TC_A_BYTES + TC_B_BYTES));
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
                 const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 16 bf16 = 32 B along K
@@ -237,7 +243,7 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
     __syncthreads();
     if (!s_fail && nkb > 0) {
         const int row = t0 + warp * 32 + lane;
-        float* out = part + ((size_t)blockIdx.z * T_pad + row) * E_pad + e0;
+        float* out = part + ((size_t)blockIdx.z * T_pad + row) * part_cols + e0;
 #pragma unroll 1
         for (int c = 0; c < TC_BN / 32; ++c) {
             uint32_t r[32];
@@ -250,7 +256,7 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
         }
     } else if (nkb == 0) {
         const int row = t0 + warp * 32 + lane;
-        float* out = part + ((size_t)blockIdx.z * T_pad + row) * E_pad + e0;
+        float* out = part + ((size_t)blockIdx.z * T_pad + row) * part_cols + e0;
         for (int c = 0; c < TC_BN; ++c) out[c] = 0.0f;
     }
     if (s_fail && threadIdx.x == 0) atomicExch(err, 1);
@@ -263,13 +269,13 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
 }
 
 // egm[t][e] = sum_z part[z][t][e] (split order, FP64), t < T, e < n_e.
-__global__ void tc_reduce_kernel(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int splits,
+__global__ void tc_reduce_kernel(int64_t T, int64_t n_e, int64_t T_pad, int64_t part_cols, int splits,
                                  const float* __restrict__ part, float* __restrict__ egm) {
     const int64_t total = T * n_e;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t t = i / n_e, e = i % n_e;
         double s = 0.0;
-        for (int z = 0; z < splits; ++z) s += (double)part[((size_t)z * T_pad + t) * E_pad + e];
+        for (int z = 0; z < splits; ++z) s += (double)part[((size_t)z * T_pad + t) * part_cols + e];
         egm[i] = (float)s;
     }
 }
@@ -306,12 +312,14 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k) {
+// Tensor map of a [rows][cols_k] BF16 operand, boxes of box_rows x 64 (rows
+// past the end read as zeros).
+bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k, int box_rows) {
     auto enc = get_encode();
     if (!enc) return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols_k, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols_k * 2};
-    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)TC_BM};
+    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -325,11 +333,14 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k) {
 // each accumulator is kept short and the slices are summed in FP64.
 constexpr int64_t kMaxKBlocksPerSplit = 128;
 
+// Columns of the split-K partial tiles: n_e_pad rounded up to the tile width.
+int64_t partial_cols(int64_t E_pad) { return (E_pad + TC_BN - 1) / TC_BN * TC_BN; }
+
 void splits_for(int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* kb_per) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t tiles = (T_pad / TC_BM) * (E_pad / TC_BN);
+    const int64_t tiles = (T_pad / TC_BM) * (partial_cols(E_pad) / TC_BN);
     const int64_t nkb = K_pad / TC_BK;
     int64_t s = std::max<int64_t>(1, (4LL * sms + tiles - 1) / tiles);
     s = std::max<int64_t>(s, (nkb + kMaxKBlocksPerSplit - 1) / kMaxKBlocksPerSplit);
@@ -347,7 +358,7 @@ int64_t bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad) {
     if (T_pad <= 0 || n_e_pad <= 0 || K_pad <= 0) return -1;
     int s = 1, per = 1;
     splits_for(T_pad, n_e_pad, K_pad, &s, &per);
-    return kTcHeader + (int64_t)s * T_pad * n_e_pad * 4;
+    return kTcHeader + (int64_t)s * T_pad * partial_cols(n_e_pad) * 4;
 }
 
 int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src_f64, uint16_t* hi, uint16_t* lo,
@@ -367,15 +378,16 @@ int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src
 int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int64_t K_pad, const uint16_t* Vhi,
                     const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo, float* egm, void* work,
                     cudaStream_t stream) {
-    if (T <= 0 || n_e <= 0 || T > T_pad || n_e > E_pad || T_pad % TC_BM || E_pad % TC_BN || K_pad % TC_BK ||
+    if (T <= 0 || n_e <= 0 || T > T_pad || n_e > E_pad || T_pad % TC_BM || E_pad % 128 || K_pad % TC_BK ||
         K_pad <= 0 || !Vhi || !Vlo || !Mhi || !Mlo || !egm || !work)
         return PHS_ERR_BAD_ARG;
-    if (T_pad / TC_BM > 65535 || E_pad / TC_BN > 65535 || K_pad / TC_BK > INT32_MAX) return PHS_ERR_BAD_ARG;
+    const int64_t Ew = partial_cols(E_pad);
+    if (T_pad / TC_BM > 65535 || Ew / TC_BN > 65535 || K_pad / TC_BK > INT32_MAX) return PHS_ERR_BAD_ARG;
     // 16-byte aligned bases and row strides for TMA
     if (((uintptr_t)Vhi | (uintptr_t)Vlo | (uintptr_t)Mhi | (uintptr_t)Mlo) & 15) return PHS_ERR_BAD_ARG;
     CUtensorMap mv_hi, mv_lo, mm_hi, mm_lo;
-    if (!make_map(&mv_hi, Vhi, T_pad, K_pad) || !make_map(&mv_lo, Vlo, T_pad, K_pad) ||
-        !make_map(&mm_hi, Mhi, E_pad, K_pad) || !make_map(&mm_lo, Mlo, E_pad, K_pad))
+    if (!make_map(&mv_hi, Vhi, T_pad, K_pad, TC_BM) || !make_map(&mv_lo, Vlo, T_pad, K_pad, TC_BM) ||
+        !make_map(&mm_hi, Mhi, E_pad, K_pad, TC_BN) || !make_map(&mm_lo, Mlo, E_pad, K_pad, TC_BN))
         return PHS_ERR_CUDA;
     int splits = 1, per = 1;
     splits_for(T_pad, E_pad, K_pad, &splits, &per);
@@ -395,13 +407,13 @@ int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int64_
             if (dev >= 0 && dev < 64) attr_set[dev] = true;
         }
     }
-    dim3 grid((unsigned)(T_pad / TC_BM), (unsigned)(E_pad / TC_BN), (unsigned)splits);
+    dim3 grid((unsigned)(T_pad / TC_BM), (unsigned)(Ew / TC_BN), (unsigned)splits);
     egm_bf16x3_kernel<<<grid, TC_THREADS, TC_SMEM, stream>>>(mv_hi, mv_lo, mm_hi, mm_lo, (int)(K_pad / TC_BK), per,
-                                                             (int)T_pad, (int)E_pad, part, err);
+                                                             (int)T_pad, (int)Ew, part, err);
     PHS_CUDA_TRY(cudaGetLastError());
     const int64_t total = T * n_e;
     tc_reduce_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 8192), 256, 0, stream>>>(
-        T, n_e, T_pad, E_pad, splits, part, egm);
+        T, n_e, T_pad, Ew, splits, part, egm);
     PHS_CUDA_TRY(cudaGetLastError());
     return PHS_OK;
 }
