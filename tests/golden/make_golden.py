@@ -1,9 +1,10 @@
 """Generate the golden fixtures in ``tests/golden/*.npz`` by running the
 reference's OWN, unmodified code in this container.
 
-Test infrastructure only.  Needs the reference checkout (``/root/reference``),
-which exists only where the fixtures are generated; the fixtures themselves are
-committed and nothing at test time reads the reference.
+Test infrastructure only.  Needs a checkout of the reference, named by the
+environment variable ``PHS_REFERENCE_DIR``; it exists only where the fixtures
+are generated, the fixtures themselves are committed and nothing at test time
+reads the reference.
 
 How the reference runs without CuPy or a GPU:
 
@@ -22,7 +23,7 @@ The neighbour tables come from the reference's own
 ``utility/voxelization.py::find_neighbor_voxel_ids`` (KDTree on integer
 coordinates), loaded with stub modules for its plotting imports.
 
-Run:  python tests/golden/make_golden.py   (a few minutes)
+Run:  PHS_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py   (a few minutes)
 """
 import importlib.util
 import os
@@ -34,7 +35,7 @@ os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
 
 import numpy as np  # noqa: E402
 
-REF = os.environ.get("PHS_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("PHS_REFERENCE_DIR", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 import cupy_standin  # noqa: E402
@@ -178,6 +179,8 @@ def _pack(prefix, d):
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "simulation")):
+        raise SystemExit("set PHS_REFERENCE_DIR to a checkout of the reference")
     cp, simulation, vox = _load_reference()
     import io
     import contextlib
