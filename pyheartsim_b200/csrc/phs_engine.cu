@@ -351,7 +351,12 @@ __device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
 }
 
-constexpr int kChunk = 4;  // basis vectors whose loads are issued together
+// Basis vectors whose loads are issued together: FP32 tiles hold four voxels
+// per thread (four loads per vector already), FP64 tiles one, and the FP64
+// plain form's GMRES(50) cycles pass over up to 50 vectors per phase, so its
+// chunks are four times longer to keep as many loads in flight.
+template <typename T>
+constexpr int kChunkOf = sizeof(T) == 8 ? 16 : 4;
 template <typename T>
 constexpr bool kWarpParts = sizeof(T) == 4;
 
@@ -363,6 +368,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_map,
             long long n_steps_launch, unsigned int* abort_word) {
     constexpr int TILE = kThreads * VPT;
+    constexpr int kChunk = kChunkOf<T>;
     const int4 cm = cta_map[blockIdx.x];
     const int rank = cm.y;
     const int P = cm.z;
@@ -930,8 +936,10 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                                 double d = 0.0;
 #pragma unroll
                                 for (int v = 0; v < VPT; ++v) d += (double)vv[ii][v] * (double)wr[v];
-                                d = warp_sum(d);
-                                if (i0 + ii <= j) put(tile, i0 + ii, d);
+                                if (i0 + ii <= j) {          // uniform over the warp
+                                    d = warp_sum(d);
+                                    put(tile, i0 + ii, d);
+                                }
                             }
                         }
                         tile_done(tile, j + 1);
