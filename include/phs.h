@@ -225,6 +225,13 @@ int64_t phs_egm_bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
 int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
                             const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi,
                             const uint16_t* Mlo, float* egm, void* work, void* stream);
+/* phs_egm_contract_bf16x3 with a tile configuration, 0 .. count-1 (output tile
+ * 128 x 128 or 128 x 256, K blocks of 64 or 32 per pipeline stage); the
+ * workspace size above covers every configuration.  For the autotuner.         */
+int phs_egm_contract_bf16x3_cfg(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
+                                const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi,
+                                const uint16_t* Mlo, float* egm, void* work, int config, void* stream);
+int phs_egm_bf16x3_config_count(void);
 /* Synchronise `stream` and read the error word of the last contraction that used
  * `work`: PHS_OK, or PHS_ERR_TIMEOUT when its pipeline waits gave up.          */
 int phs_egm_bf16x3_status(const void* work, void* stream);

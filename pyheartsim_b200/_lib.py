@@ -171,6 +171,11 @@ SIGNATURES = {
                                                ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "phs_egm_bf16x3_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "phs_egm_contract_bf16x3_cfg": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                                   ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_void_p]),
+    "phs_egm_bf16x3_config_count": (ctypes.c_int, []),
     "phs_egm_contract_f64_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                                     ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_void_p]),

@@ -225,7 +225,8 @@ int normalize(int64_t T, int64_t n_e, void* egm, bool is_f64, cudaStream_t strea
 // defined in phs_egm_tc.cu
 int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
                     const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo,
-                    float* egm, void* work, cudaStream_t stream);
+                    float* egm, void* work, cudaStream_t stream, int config);
+int bf16x3_config_count();
 int64_t bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad);
 int bf16x3_status(const void* work, cudaStream_t stream);
 int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src_f64, uint16_t* hi,
@@ -274,8 +275,18 @@ int64_t phs_egm_bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad) 
 int phs_egm_contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
                             const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo,
                             float* egm, void* work, void* stream) {
-    return contract_bf16x3(T, n_e, T_pad, n_e_pad, K_pad, Vhi, Vlo, Mhi, Mlo, egm, work, (cudaStream_t)stream);
+    return contract_bf16x3(T, n_e, T_pad, n_e_pad, K_pad, Vhi, Vlo, Mhi, Mlo, egm, work, (cudaStream_t)stream, -1);
 }
+
+int phs_egm_contract_bf16x3_cfg(int64_t T, int64_t n_e, int64_t T_pad, int64_t n_e_pad, int64_t K_pad,
+                                const uint16_t* Vhi, const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo,
+                                float* egm, void* work, int config, void* stream) {
+    if (config < 0) return PHS_ERR_BAD_ARG;
+    return contract_bf16x3(T, n_e, T_pad, n_e_pad, K_pad, Vhi, Vlo, Mhi, Mlo, egm, work, (cudaStream_t)stream,
+                           config);
+}
+
+int phs_egm_bf16x3_config_count(void) { return bf16x3_config_count(); }
 
 int phs_egm_bf16x3_status(const void* work, void* stream) { return bf16x3_status(work, (cudaStream_t)stream); }
 
@@ -340,7 +351,7 @@ int phs_electrogram(int64_t T, int64_t n_v, int64_t n_e, const double* V, const 
         if (!vh || !vl || !mh || !ml || !e32 || !work) return cleanup(PHS_ERR_OOM);
         rc = split_bf16(T, n_v, dV, n_v, true, vh, vl, Tp, Kp, s);
         if (rc == PHS_OK) rc = split_bf16(n_e, n_v, dMt, n_v, true, mh, ml, Ep, Kp, s);
-        if (rc == PHS_OK) rc = contract_bf16x3(T, n_e, Tp, Ep, Kp, vh, vl, mh, ml, e32, work, s);
+        if (rc == PHS_OK) rc = contract_bf16x3(T, n_e, Tp, Ep, Kp, vh, vl, mh, ml, e32, work, s, -1);
         if (rc == PHS_OK) rc = bf16x3_status(work, s);
         if (rc == PHS_OK) rc = normalize(T, n_e, e32, false, s);
         if (rc == PHS_OK) {

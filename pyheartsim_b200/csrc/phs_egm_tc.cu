@@ -8,18 +8,22 @@
 // simulation/unipolar_electrogram_gpu.py:21-69 by a dense contraction of the
 // lead field (see phs_egm.cu) against the Vm history.
 //
-// One CTA computes a 128 (t) x 256 (e) tile over one K range (split-K):
-//   warp 0 lane 0   TMA producer: per stage two 128x64 BF16 tiles of V (hi, lo)
-//                   and two 256x64 tiles of M (hi, lo), 128-byte swizzle,
-//                   2-stage mbarrier ring (96 KB per stage)
-//   warp 1 lane 0   MMA issuer: per 64-wide K block, 4 K-slices x 3 products of
-//                   tcgen05.mma.cta_group::1.kind::f16 (M=128, N=256, K=16) into
-//                   one FP32 accumulator in TMEM (256 columns); tcgen05.commit
-//                   frees the stage
+// One CTA computes a 128 (t) x BN (e) tile over one K range (split-K):
+//   warp 0 lane 0   TMA producer: per stage two 128 x BK BF16 tiles of V (hi,
+//                   lo) and two BN x BK tiles of M (hi, lo), 128-byte (BK = 64)
+//                   or 64-byte (BK = 32) swizzle, an mbarrier ring of STAGES
+//   warp 1 lane 0   MMA issuer: per BK-wide K block, BK/16 K-slices x 3 products
+//                   of tcgen05.mma.cta_group::1.kind::f16 (M=128, N=BN, K=16)
+//                   into one FP32 accumulator in TMEM (BN columns);
+//                   tcgen05.commit frees the stage
 //   warps 0..3      epilogue: tcgen05.ld 32x32b.x32 -> FP32 partial tile in HBM
-// The 256-wide tile reads 96 KB of operands per 2 x 128 x 256 x 64 x 3 FLOPs,
-// 0.75 of what two 128 x 128 tiles read: the contraction streams its operands
-// from L2, so fewer bytes per FLOP keep the tensor pipe busier.
+// Tile configurations (kTcConfigs; every one uses 192 KB of shared memory):
+// 128 x 128 with 3 stages of BK 64, 128 x 256 with 2 stages of BK 64, 128 x 256
+// with 4 stages of BK 32, 128 x 128 with 6 stages of BK 32.  The 256-wide tiles
+// read 0.75 of the operand bytes per FLOP of the 128-wide ones (the operands
+// stream from L2); the BK-32 rings keep more, smaller stages in flight ahead of
+// the MMAs.  phs_egm_contract_bf16x3 uses kTcDefaultConfig;
+// phs_egm_contract_bf16x3_cfg takes a configuration (the autotuner's choice).
 // Split-K partials are summed in split order by a second kernel.
 //
 // Every wait is bounded (kTcWaitNs); on timeout the CTA records an error word,
@@ -38,15 +42,19 @@
 namespace phs {
 
 constexpr int TC_BM = 128;
-constexpr int TC_BN = 256;
-constexpr int TC_BK = 64;                       // 64 bf16 = 128 B rows (one swizzle atom)
-constexpr int TC_STAGES = 2;
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;   // 16 KB
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;   // 32 KB
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
+constexpr int TC_BN_MAX = 256;
 constexpr int TC_THREADS = 128;
-constexpr int TC_TMEM_COLS = TC_BN;
-constexpr size_t TC_SMEM = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+
+// Compile-time shape of one tile configuration.
+template <int BN, int BK, int STAGES>
+struct TcShape {
+    static constexpr int A_BYTES = TC_BM * BK * 2;
+    static constexpr int B_BYTES = BN * BK * 2;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr size_t SMEM = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr uint32_t SBO = 8u * BK * 2u;            // bytes between 8-row core-matrix groups
+    static constexpr uint64_t LAYOUT = BK == 64 ? 2u : 4u;   // SWIZZLE_128B / SWIZZLE_64B
+};
 constexpr unsigned long long kTcWaitNs = 2000000000ull;  // 2 s
 constexpr int64_t kTcHeader = 256;                        // error word at the workspace head
 
@@ -96,14 +104,15 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+// UMMA shared-memory descriptor: K-major, swizzled rows (128 or 64 bytes), 8-row
+// groups `sbo` bytes apart.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t sbo, uint64_t layout) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFFu);        // start address
-    d |= (uint64_t)1u << 16;                          // leading byte offset (unused for SW128 K-major)
-    d |= (uint64_t)(1024u >> 4) << 32;               // stride byte offset
+    d |= (uint64_t)1u << 16;                          // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;     // stride byte offset
     d |= (uint64_t)1u << 46;                          // descriptor version (sm_100)
-    d |= (uint64_t)2u << 61;                          // SWIZZLE_128B
+    d |= layout << 61;                                // swizzle mode
     return d;
 }
 
@@ -143,11 +152,20 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+template <int BN, int BK, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_constant__ CUtensorMap map_vlo,
                   const __grid_constant__ CUtensorMap map_mhi, const __grid_constant__ CUtensorMap map_mlo,
                   int nkb_total, int kb_per_split, int T_pad, int part_cols, float* __restrict__ part,
                   int* __restrict__ err) {
+    using Sh = TcShape<BN, BK, STAGES>;
+    constexpr int TC_BN = BN;
+    constexpr int TC_BK = BK;
+    constexpr int TC_STAGES = STAGES;
+    constexpr int TC_A_BYTES = Sh::A_BYTES;
+    constexpr int TC_B_BYTES = Sh::B_BYTES;
+    constexpr int TC_STAGE_BYTES = Sh::STAGE_BYTES;
+    constexpr int TC_TMEM_COLS = BN;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)tc_smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* bars = (uint64_t*)(smem + (size_t)TC_STAGES * TC_STAGE_BYTES);
@@ -218,10 +236,10 @@ egm_bf16x3_kernel(const __grid_constant__ CUtensorMap map_vhi, const __grid_cons
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint8_t* st = smem + (size_t)s * TC_STAGE_BYTES;
-            const uint64_t dAh = umma_desc_sw128(smem_u32(st));
-            const uint64_t dAl = umma_desc_sw128(smem_u32(st + TC_A_BYTES));
-            const uint64_t dBh = umma_desc_sw128(smem_u32(st + 2 * TC_A_BYTES));
-            const uint64_t dBl = umma_desc_sw128(smem_u32(st + 2 * TC_A_BYTES + TC_B_BYTES));
+            const uint64_t dAh = umma_desc(smem_u32(st), Sh::SBO, Sh::LAYOUT);
+            const uint64_t dAl = umma_desc(smem_u32(st + TC_A_BYTES), Sh::SBO, Sh::LAYOUT);
+            const uint64_t dBh = umma_desc(smem_u32(st + 2 * TC_A_BYTES), Sh::SBO, Sh::LAYOUT);
+            const uint64_t dBl = umma_desc(smem_u32(st + 2 * TC_A_BYTES + TC_B_BYTES), Sh::SBO, Sh::LAYOUT);
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
                 const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 16 bf16 = 32 B along K
@@ -312,38 +330,54 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
     return fn;
 }
 
-// Tensor map of a [rows][cols_k] BF16 operand, boxes of box_rows x 64 (rows
-// past the end read as zeros).
-bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k, int box_rows) {
+// Tensor map of a [rows][cols_k] BF16 operand, boxes of box_rows x bk (rows
+// past the end read as zeros), swizzled to match the MMA descriptors.
+bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t cols_k, int box_rows, int bk) {
     auto enc = get_encode();
     if (!enc) return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols_k, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols_k * 2};
-    cuuint32_t box[2] = {(cuuint32_t)TC_BK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)bk, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
-// Split-K: at least ~4 CTAs per SM, and at most kMaxKBlocksPerSplit K blocks
+// Split-K: at least ~4 CTAs per SM, and at most kMaxKPerSplit K values
 // accumulated in one FP32 TMEM accumulator.  Long FP32 accumulation chains are
 // the dominant error of the split-BF16 contraction (the dipole sum cancels), so
 // each accumulator is kept short and the slices are summed in FP64.
-constexpr int64_t kMaxKBlocksPerSplit = 128;
+constexpr int64_t kMaxKPerSplit = 8192;
+
+// The tile configurations: (BN, BK, stages), their kernels and shared memory.
+struct TcConfig {
+    int bn, bk, stages;
+    const void* fn;
+    size_t smem;
+};
+template <int BN, int BK, int ST>
+constexpr TcConfig tc_config() {
+    return TcConfig{BN, BK, ST, (const void*)egm_bf16x3_kernel<BN, BK, ST>, TcShape<BN, BK, ST>::SMEM};
+}
+const TcConfig kTcConfigs[] = {tc_config<128, 64, 3>(), tc_config<256, 64, 2>(), tc_config<256, 32, 4>(),
+                               tc_config<128, 32, 6>()};
+constexpr int kTcNumConfigs = 4;
+constexpr int kTcDefaultConfig = 0;
 
 // Columns of the split-K partial tiles: n_e_pad rounded up to the tile width.
-int64_t partial_cols(int64_t E_pad) { return (E_pad + TC_BN - 1) / TC_BN * TC_BN; }
+int64_t partial_cols(int64_t E_pad, int bn) { return (E_pad + bn - 1) / bn * bn; }
 
-void splits_for(int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* kb_per) {
+void splits_for(const TcConfig& c, int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* kb_per) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t tiles = (T_pad / TC_BM) * (partial_cols(E_pad) / TC_BN);
-    const int64_t nkb = K_pad / TC_BK;
+    const int64_t tiles = (T_pad / TC_BM) * (partial_cols(E_pad, c.bn) / c.bn);
+    const int64_t nkb = K_pad / c.bk;
+    const int64_t max_kb = kMaxKPerSplit / c.bk;
     int64_t s = std::max<int64_t>(1, (4LL * sms + tiles - 1) / tiles);
-    s = std::max<int64_t>(s, (nkb + kMaxKBlocksPerSplit - 1) / kMaxKBlocksPerSplit);
+    s = std::max<int64_t>(s, (nkb + max_kb - 1) / max_kb);
     s = std::min<int64_t>(s, std::max<int64_t>(1, nkb / 8));
     s = std::min<int64_t>(s, 65535);
     int64_t per = (nkb + s - 1) / s;
@@ -352,13 +386,21 @@ void splits_for(int64_t T_pad, int64_t E_pad, int64_t K_pad, int* splits, int* k
     *kb_per = (int)per;
 }
 
+int64_t workspace_of(const TcConfig& c, int64_t T_pad, int64_t E_pad, int64_t K_pad) {
+    int s = 1, per = 1;
+    splits_for(c, T_pad, E_pad, K_pad, &s, &per);
+    return kTcHeader + (int64_t)s * T_pad * partial_cols(E_pad, c.bn) * 4;
+}
+
 }  // namespace
+
+int bf16x3_config_count() { return kTcNumConfigs; }
 
 int64_t bf16x3_workspace(int64_t T_pad, int64_t n_e_pad, int64_t K_pad) {
     if (T_pad <= 0 || n_e_pad <= 0 || K_pad <= 0) return -1;
-    int s = 1, per = 1;
-    splits_for(T_pad, n_e_pad, K_pad, &s, &per);
-    return kTcHeader + (int64_t)s * T_pad * partial_cols(n_e_pad) * 4;
+    int64_t w = 0;
+    for (const TcConfig& c : kTcConfigs) w = std::max(w, workspace_of(c, T_pad, n_e_pad, K_pad));
+    return w;
 }
 
 int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src_f64, uint16_t* hi, uint16_t* lo,
@@ -377,40 +419,43 @@ int split_bf16(int64_t rows, int64_t cols, const void* src, int64_t ld, bool src
 
 int contract_bf16x3(int64_t T, int64_t n_e, int64_t T_pad, int64_t E_pad, int64_t K_pad, const uint16_t* Vhi,
                     const uint16_t* Vlo, const uint16_t* Mhi, const uint16_t* Mlo, float* egm, void* work,
-                    cudaStream_t stream) {
-    if (T <= 0 || n_e <= 0 || T > T_pad || n_e > E_pad || T_pad % TC_BM || E_pad % 128 || K_pad % TC_BK ||
+                    cudaStream_t stream, int config) {
+    if (config < 0) config = kTcDefaultConfig;
+    if (config >= kTcNumConfigs) return PHS_ERR_BAD_ARG;
+    const TcConfig& c = kTcConfigs[config];
+    if (T <= 0 || n_e <= 0 || T > T_pad || n_e > E_pad || T_pad % TC_BM || E_pad % 128 || K_pad % 64 ||
         K_pad <= 0 || !Vhi || !Vlo || !Mhi || !Mlo || !egm || !work)
         return PHS_ERR_BAD_ARG;
-    const int64_t Ew = partial_cols(E_pad);
-    if (T_pad / TC_BM > 65535 || Ew / TC_BN > 65535 || K_pad / TC_BK > INT32_MAX) return PHS_ERR_BAD_ARG;
+    const int64_t Ew = partial_cols(E_pad, c.bn);
+    if (T_pad / TC_BM > 65535 || Ew / c.bn > 65535 || K_pad / c.bk > INT32_MAX) return PHS_ERR_BAD_ARG;
     // 16-byte aligned bases and row strides for TMA
     if (((uintptr_t)Vhi | (uintptr_t)Vlo | (uintptr_t)Mhi | (uintptr_t)Mlo) & 15) return PHS_ERR_BAD_ARG;
     CUtensorMap mv_hi, mv_lo, mm_hi, mm_lo;
-    if (!make_map(&mv_hi, Vhi, T_pad, K_pad, TC_BM) || !make_map(&mv_lo, Vlo, T_pad, K_pad, TC_BM) ||
-        !make_map(&mm_hi, Mhi, E_pad, K_pad, TC_BN) || !make_map(&mm_lo, Mlo, E_pad, K_pad, TC_BN))
+    if (!make_map(&mv_hi, Vhi, T_pad, K_pad, TC_BM, c.bk) || !make_map(&mv_lo, Vlo, T_pad, K_pad, TC_BM, c.bk) ||
+        !make_map(&mm_hi, Mhi, E_pad, K_pad, c.bn, c.bk) || !make_map(&mm_lo, Mlo, E_pad, K_pad, c.bn, c.bk))
         return PHS_ERR_CUDA;
     int splits = 1, per = 1;
-    splits_for(T_pad, E_pad, K_pad, &splits, &per);
+    splits_for(c, T_pad, E_pad, K_pad, &splits, &per);
     int* err = (int*)work;
     float* part = (float*)((char*)work + kTcHeader);
     PHS_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream));
-    // the dynamic shared-memory opt-in is a per-device attribute of the kernel
+    // the dynamic shared-memory opt-in is a per-device attribute of each kernel
     {
         static std::mutex mu;
-        static bool attr_set[64] = {};
+        static bool attr_set[64][kTcNumConfigs] = {};
         int dev = 0;
         PHS_CUDA_TRY(cudaGetDevice(&dev));
         std::lock_guard<std::mutex> lk(mu);
-        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-            PHS_CUDA_TRY(cudaFuncSetAttribute(egm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)TC_SMEM));
-            if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        if (dev < 0 || dev >= 64 || !attr_set[dev][config]) {
+            PHS_CUDA_TRY(cudaFuncSetAttribute(c.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+            if (dev >= 0 && dev < 64) attr_set[dev][config] = true;
         }
     }
-    dim3 grid((unsigned)(T_pad / TC_BM), (unsigned)(Ew / TC_BN), (unsigned)splits);
-    egm_bf16x3_kernel<<<grid, TC_THREADS, TC_SMEM, stream>>>(mv_hi, mv_lo, mm_hi, mm_lo, (int)(K_pad / TC_BK), per,
-                                                             (int)T_pad, (int)Ew, part, err);
-    PHS_CUDA_TRY(cudaGetLastError());
+    dim3 grid((unsigned)(T_pad / TC_BM), (unsigned)(Ew / c.bn), (unsigned)splits);
+    int nkb_total = (int)(K_pad / c.bk), T_pad_i = (int)T_pad, Ew_i = (int)Ew;
+    void* args[] = {(void*)&mv_hi, (void*)&mv_lo, (void*)&mm_hi, (void*)&mm_lo, (void*)&nkb_total, (void*)&per,
+                    (void*)&T_pad_i, (void*)&Ew_i, (void*)&part, (void*)&err};
+    PHS_CUDA_TRY(cudaLaunchKernel(c.fn, grid, dim3(TC_THREADS), args, c.smem, stream));
     const int64_t total = T * n_e;
     tc_reduce_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 8192), 256, 0, stream>>>(
         T, n_e, T_pad, Ew, splits, part, egm);

@@ -87,9 +87,12 @@ def test_egm_bf16x3_rel_l2(cuda_device):
     assert r < BF16X3_REL_L2, r
 
 
+@pytest.mark.parametrize("config", [-1, 0, 1, 2, 3])
 @pytest.mark.parametrize("T,K,E", [(77, 5000, 40), (256, 8192, 256), (300, 20000, 130)])
-def test_bf16x3_contraction_device_pointers(T, K, E, cuda_device):
-    """The tcgen05 kernel alone, on torch-owned device buffers."""
+def test_bf16x3_contraction_device_pointers(T, K, E, config, cuda_device):
+    """The tcgen05 kernel alone, on torch-owned device buffers, in every tile
+    configuration (-1: the default entry point); E = 40 and 130 pad to 128 and
+    256 rows, so the 256-wide tiles also read rows past the operand's end."""
     import torch
     g = torch.Generator(device="cpu").manual_seed(T + K + E)
     A = torch.randn(T, K, dtype=torch.float64, generator=g)
@@ -109,8 +112,13 @@ def test_bf16x3_contraction_device_pointers(T, K, E, cuda_device):
     ws = L.phs_egm_bf16x3_workspace(Tp, Ep, Kp)
     work = torch.empty(ws, dtype=torch.uint8, device=cuda_device)
     out = torch.empty(T, E, dtype=torch.float32, device=cuda_device)
-    _lib.check(L.phs_egm_contract_bf16x3(T, E, Tp, Ep, Kp, p(hA), p(lA), p(hB), p(lB), p(out), p(work), s),
-               "contract")
+    assert L.phs_egm_bf16x3_config_count() == 4
+    if config < 0:
+        _lib.check(L.phs_egm_contract_bf16x3(T, E, Tp, Ep, Kp, p(hA), p(lA), p(hB), p(lB), p(out), p(work), s),
+                   "contract")
+    else:
+        _lib.check(L.phs_egm_contract_bf16x3_cfg(T, E, Tp, Ep, Kp, p(hA), p(lA), p(hB), p(lB), p(out), p(work),
+                                                 config, s), "contract")
     _lib.check(L.phs_egm_bf16x3_status(p(work), s), "contract status")
     torch.cuda.synchronize()
     got = out.cpu().numpy().astype(np.float64)
