@@ -178,12 +178,14 @@ def sheet_c1(nx=200, ny=200, t_phys=500.0):
 
 
 # Pacing of the rotor shell per wall thickness: (S1 depth in mm, S1-S2 coupling
-# interval in physical ms).  Chosen by sweeps of the FP32 engine over the
-# coupling interval: the S1 plane must fire on its own (a 1.2 mm cap fires
-# through a 3-voxel wall but not through an 8-voxel one, whose thicker wall
-# drains it), and the S2 quadrant must land on the S1 wave's refractory tail
-# so that re-entry runs to the end of the 1000 ms run.
-C2_PACING = {3: (1.2, 240.0), 8: (2.4, 240.0)}
+# interval in physical ms).  Chosen by sweeps of the FP32 engine: the S1 cap
+# must fire on its own (1.2 mm fires through a 3-voxel wall but not through an
+# 8-voxel one, which drains it; 2.4 mm fires), and S2 must land on the S1 wave's
+# refractory tail.  Wall 3 with a 1.2 mm cap sustains re-entry to the end of
+# the 1000 ms run (up to 6 activations per voxel) for S1-S2 of 220-240 ms and
+# not from 250 ms; wall 8 with a 2.4 mm cap for 220 ms only (200 ms: S2 does not
+# take; 240-300 ms: one extra wave that dies by 425 ms).
+C2_PACING = {3: (1.2, 240.0), 8: (2.4, 220.0)}
 
 
 def atrium_c2(wall=3, seed=0, t_phys=1000.0, s1_s2=None, n_electrodes=64, s1_mm=None):
