@@ -114,6 +114,8 @@ struct InstDev {
     T* hist_h;              // [S*n] or nullptr
     int32_t* lat;           // [n]
     double* part;           // [n_tiles*kSlots]
+    double* gpart;          // FP64: [n_groups*kSlots] sums of kGroupTiles consecutive tiles, or nullptr
+    unsigned int* gcnt;     // FP64: [n_groups] arrivals of the current phase at each group
     Scalars* sc;
     TeamSync* sync;
     InstState* st;
@@ -125,6 +127,7 @@ struct InstDev {
     long long n_steps;
     long long tb_steps;
     int n_tiles;
+    int n_groups;           // ceil(n_tiles / kGroupTiles)
     int ps;                 // partial slots per (tile, warp): m + 2
     int model;
     int m;                  // restart length actually used: min(restart, n)
@@ -359,6 +362,10 @@ template <typename T>
 constexpr int kChunkOf = sizeof(T) == 8 ? 16 : 4;
 template <typename T>
 constexpr bool kWarpParts = sizeof(T) == 4;
+// FP64 partial sums are combined in fixed groups of this many consecutive tiles
+// by whichever CTA finishes a group's last tile, so the leader reads one
+// partial per group (GMRES(50) reduces up to 51 slots per barrier).
+constexpr int kGroupTiles = 8;
 
 // ------------------------------------------------------------------ the kernel
 // EDGE: the launch carries anisotropic instances (edge cross terms); the
@@ -391,7 +398,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     const long long N = I.n;
     const int ps = I.ps;
-    const int nparts = kWarpParts<T> ? I.n_tiles * kWarps : I.n_tiles;
+    const int nparts = kWarpParts<T> ? I.n_tiles * kWarps : I.n_groups;
+    const double* psum = kWarpParts<T> ? I.part : I.gpart;   // what the leader sums
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     Scalars* sc = I.sc;
@@ -432,6 +440,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             if (lane == 0) red[red_buf][warp][slot] = v;
         }
     };
+    __shared__ int sh_glast;
     auto tile_done = [&](int tile, int nslot) {
         if constexpr (!kWarpParts<T>) {
             __syncthreads();
@@ -442,6 +451,28 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 I.part[(size_t)tile * ps + t] = a;
             }
             red_buf ^= 1;
+            // the CTA that completes a group of tiles sums the group, tiles in order
+            const int g = tile / kGroupTiles;
+            const int t0 = g * kGroupTiles;
+            const int t1 = min(t0 + kGroupTiles, I.n_tiles);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const unsigned int prev = atomicAdd(I.gcnt + g, 1u);
+                sh_glast = (prev == (unsigned int)(t1 - t0 - 1));
+            }
+            __syncthreads();
+            if (sh_glast) {
+                __threadfence();
+                for (int t = threadIdx.x; t < nslot; t += kThreads) {
+                    double a = 0.0;
+                    for (int q = t0; q < t1; ++q) a += __ldcg(I.part + (size_t)q * ps + t);
+                    I.gpart[(size_t)g * ps + t] = a;
+                }
+                // every tile of the group has arrived in this phase; the next
+                // phase's arrivals come after the team barrier
+                if (threadIdx.x == 0) I.gcnt[g] = 0u;
+            }
         }
     };
     auto voxel = [&](int tile, int v) -> long long { return (long long)tile * TILE + v * kThreads + threadIdx.x; };
@@ -503,7 +534,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             for (int u = 0; u < kSumW; ++u) a[u] = 0.0;
 #pragma unroll 4
             for (int q = threadIdx.x; q < nparts; q += kThreads) {
-                const double* pq = I.part + (size_t)q * ps + slot0 + s0;
+                const double* pq = psum + (size_t)q * ps + slot0 + s0;
 #pragma unroll
                 for (int u = 0; u < kSumW; ++u)
                     if (s0 + u < ns) a[u] += __ldcg(pq + u);
@@ -1252,6 +1283,9 @@ struct InstHost {
     void* hist_h = nullptr;
     int32_t* lat = nullptr;
     double* part = nullptr;
+    double* gpart = nullptr;
+    unsigned int* gcnt = nullptr;
+    int n_groups = 0;
     Scalars* sc = nullptr;
     TeamSync* sync = nullptr;
     InstState* st = nullptr;
@@ -1267,7 +1301,7 @@ struct InstHost {
 
 void free_inst(InstHost& h) {
     void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.enb, h.ecf, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
-                    h.hist_u, h.hist_h, h.lat, h.part, h.sc, h.sync, h.st, h.prof};
+                    h.hist_u, h.hist_h, h.lat, h.part, h.gpart, h.gcnt, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     h = InstHost();
@@ -1475,6 +1509,11 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     PHS_ALLOC(h.lat, n * sizeof(int32_t));
     const size_t nparts = (size_t)h.n_tiles * (kWarpParts<T> ? kWarps : 1);
     PHS_ALLOC(h.part, nparts * (h.m + 2) * sizeof(double));
+    h.n_groups = (h.n_tiles + kGroupTiles - 1) / kGroupTiles;
+    if (!kWarpParts<T>) {
+        PHS_ALLOC(h.gpart, (size_t)h.n_groups * (h.m + 2) * sizeof(double));
+        PHS_ALLOC(h.gcnt, (size_t)h.n_groups * sizeof(unsigned int));
+    }
     PHS_ALLOC(h.sc, sizeof(Scalars));
     PHS_ALLOC(h.sync, sizeof(TeamSync));
     PHS_ALLOC(h.st, sizeof(InstState));
@@ -1490,6 +1529,8 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     if (h.hist_h) cudaMemset(h.hist_h, 0, S * n * sizeof(T));
     cudaMemset(h.lat, 0xff, n * sizeof(int32_t));
     cudaMemset(h.part, 0, nparts * (h.m + 2) * sizeof(double));
+    if (h.gpart) cudaMemset(h.gpart, 0, (size_t)h.n_groups * (h.m + 2) * sizeof(double));
+    if (h.gcnt) cudaMemset(h.gcnt, 0, (size_t)h.n_groups * sizeof(unsigned int));
     cudaMemset(h.sc, 0, sizeof(Scalars));
     cudaMemset(h.sync, 0, sizeof(TeamSync));
     InstState st{};
@@ -1543,6 +1584,9 @@ InstDev<T> make_dev(const InstHost& h) {
     I.hist_h = (T*)h.hist_h;
     I.lat = h.lat;
     I.part = h.part;
+    I.gpart = h.gpart;
+    I.gcnt = h.gcnt;
+    I.n_groups = h.n_groups;
     I.sc = h.sc;
     I.sync = h.sync;
     I.st = h.st;
