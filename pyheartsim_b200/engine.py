@@ -78,6 +78,45 @@ class BatchedEngine:
             return u, inst.to_caller(h)
         return u
 
+    def history_device(self, slot, s0=0, count=None, stream=None):
+        """A copy of the instance's Vm history rows s0 .. s0+count as a new CUDA
+        tensor (count, n) in the caller's voxel order, gathered on the device
+        (the engine keeps its rows in device order).  The copy is made on
+        ``stream`` (default: the current torch stream) after the engine's
+        queued work; the instance may be removed once the stream has it."""
+        import torch
+        inst = self._inst[slot]
+        info = self.info(slot)
+        if count is None:
+            count = info["samples"] - s0
+        u = ctypes.c_void_p()
+        hist = ctypes.c_void_p()
+        lat = _lib.c_int32_p()
+        _lib.check(_lib.lib().phs_instance_device_ptrs(self._h, slot, ctypes.byref(u), ctypes.byref(hist),
+                                                       ctypes.byref(lat)), "phs_instance_device_ptrs")
+        n = int(inst.n_voxel)
+        tdt = torch.float32 if self.precision == _lib.PREC_F32 else torch.float64
+        dev = torch.device("cuda", torch.cuda.current_device())
+        esz = 4 if tdt == torch.float32 else 8
+
+        class _View:   # the engine's device rows, seen by torch without a copy
+            __cuda_array_interface__ = {"data": (hist.value + s0 * n * esz, False), "shape": (count, n),
+                                        "typestr": "<f4" if esz == 4 else "<f8", "version": 3, "strides": None}
+
+        torch.cuda.synchronize(dev)            # the engine's launches may be on any stream
+        src = torch.as_tensor(_View(), device=dev)
+        st = stream or torch.cuda.current_stream(dev)
+        with torch.cuda.stream(st):
+            if inst.inv is None:
+                out = src.clone()
+            else:
+                inv = getattr(inst, "_inv_dev", None)
+                if inv is None or inv.device != dev:
+                    inv = torch.as_tensor(inst.inv, device=dev)
+                    inst._inv_dev = inv
+                out = src.index_select(1, inv)
+        return out
+
     def activation_times(self, slot, max_per_voxel=16, threshold=0.5, stream=None):
         """Every upward crossing of ``threshold`` by Vm in the instance's device
         history (``phs_activation_times``): ``(times, counts)`` in the caller's

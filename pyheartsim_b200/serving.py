@@ -9,9 +9,11 @@ between launches,
 * advances every admitted instance by ``steps_per_launch`` steps in one
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
-* retires instances that reached their last step: reads the whole 1 kHz Vm
-  history back to the host (a request's latency ends when its history is
-  there), frees their device memory and lets the next request in;
+* retires instances that reached their last step: gathers the whole 1 kHz Vm
+  history into the caller's voxel order on the device, frees the instance and
+  copies the history to the host on a worker thread while the engine runs on
+  (a request's latency ends when its history is on the host; the device copy
+  counts against the budget until then);
 * re-splits CTAs over the running instances by measured cost every
   ``rebalance_every`` launches (the device phase timers run only in the launch
   before each re-split).
@@ -166,7 +168,40 @@ class Server:
         t0 = time.perf_counter()
         nxt = 0
         work = 0.0
-        while nxt < len(reqs) or queue or active:
+        # retired histories go to the host on worker threads while the engine
+        # keeps running: gathered into caller order on the device (side
+        # stream), the instance removed, the device copy counted against the
+        # budget until the host has it
+        dev_dl = hasattr(self.engine, "history_device")
+        if dev_dl:
+            import torch
+            dl_stream = torch.cuda.Stream()
+            dl_pool = ThreadPoolExecutor(max_workers=2)
+        downloads = []
+
+        def fetch(r, t):
+            with torch.cuda.stream(dl_stream):
+                hist = t.cpu().numpy()
+            r.history_bytes = hist.nbytes
+            r.history = hist if keep_history else None
+            r.done_s = time.perf_counter() - t0
+
+        def finish_downloads(block=False):
+            nonlocal downloads
+            keep = []
+            for r, fut, hold in downloads:
+                if block or fut.done():
+                    fut.result()
+                    self.used -= hold
+                    done.append(r)
+                    if log:
+                        log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
+                else:
+                    keep.append((r, fut, hold))
+            downloads = keep
+
+        while nxt < len(reqs) or queue or active or downloads:
+            finish_downloads()
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival_s * time_scale <= now:
                 queue.append(reqs[nxt])
@@ -194,6 +229,8 @@ class Server:
             if not active:
                 if nxt < len(reqs):
                     time.sleep(max(0.0, min(0.05, reqs[nxt].arrival_s * time_scale - now)))
+                elif downloads:
+                    time.sleep(0.002)
                 continue
             # phase timers only for the launch whose costs the next re-split uses
             due = (self.launches + 1) % self.rebalance_every == 0
@@ -208,17 +245,28 @@ class Server:
                 info = self.engine.info(slot)
                 if info["step"] >= info["n_steps"] or info["status"] == _lib.PHS_ERR_NONFINITE:
                     r = active.pop(slot)
+                    r.status = info["status"]
+                    work += float(r.inst.n_voxel) * info["step"]
+                    if dev_dl:
+                        t = self.engine.history_device(slot, stream=dl_stream)
+                        dl_stream.synchronize()           # the gather has read the engine's rows
+                        self.engine.remove(slot)
+                        hold = t.numel() * t.element_size()
+                        self.used += hold - r.fp
+                        downloads.append((r, dl_pool.submit(fetch, r, t), hold))
+                        continue
                     hist = self.engine.history(slot)           # the whole 1 kHz Vm history, to the host
                     r.history_bytes = hist.nbytes
                     r.history = hist if keep_history else None
-                    r.status = info["status"]
                     r.done_s = time.perf_counter() - t0
-                    work += float(r.inst.n_voxel) * info["step"]
                     self.engine.remove(slot)
                     self.used -= r.fp
                     done.append(r)
                     if log:
                         log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
+        finish_downloads(block=True)
+        if dev_dl:
+            dl_pool.shutdown()
         makespan = time.perf_counter() - t0
         return done, {"makespan_s": makespan, "voxel_steps": work, "launches": self.launches}
 
