@@ -1614,45 +1614,36 @@ InstDev<T> make_dev(const InstHost& h) {
     return I;
 }
 
-// Split G CTAs over the instances in proportion to their cost (voxels times
-// the cost of a step in units of one Arnoldi iteration: the RHS, update and
-// copy phases weigh about 1.6 iterations), at least one CTA each and never
-// more CTAs than tiles.
+// Split G CTAs over the instances.  A team of P CTAs over `tiles` tiles takes
+// time proportional to (cost per tile) x ceil(tiles / P): its CTAs walk their
+// tiles one after another and the one with the most tiles sets the pace.  The
+// cost of an instance is `weight` (voxels times the cost of a step in units of
+// one Arnoldi iteration, or the measured CTA-time per step), per tile weight /
+// tiles.  Starting from one CTA each, the instance with the longest time
+// receives the fewest CTAs that lower its tiles-per-CTA count, until the CTAs
+// run out or the longest one cannot be helped; CTAs left over (when every team
+// already has one CTA per tile, or the longest would need more than remain) go
+// to no one.  Never more CTAs than tiles.
 std::vector<int> team_sizes(const std::vector<int>& tiles, const std::vector<double>& weight, int G) {
     const int A = (int)tiles.size();
     std::vector<int> P(A, 1);
-    double total = 0.0;
-    for (double w : weight) total += w;
     int used = A;
-    for (int i = 0; i < A; ++i) {
-        long long want = (long long)((double)G * weight[i] / std::max(total, 1e-30));
-        int p = (int)std::max<long long>(1, std::min<long long>(want, tiles[i]));
-        used += p - 1;
-        P[i] = p;
-    }
+    auto per_tile = [&](int i) { return weight[i] / std::max(tiles[i], 1); };
+    auto span = [&](int i, int p) { return (tiles[i] + p - 1) / p; };
     while (used < G) {
-        int best = -1;
-        double best_ratio = 0.0;
+        int worst = -1;
+        double wt = -1.0;
         for (int i = 0; i < A; ++i) {
-            if (P[i] >= tiles[i]) continue;
-            double r = weight[i] / P[i];
-            if (r > best_ratio) { best_ratio = r; best = i; }
+            const double t = per_tile(i) * span(i, P[i]);
+            if (t > wt) { wt = t; worst = i; }
         }
-        if (best < 0) break;
-        P[best] += 1;
-        ++used;
-    }
-    while (used > G) {
-        int best = -1;
-        double best_ratio = 1e300;
-        for (int i = 0; i < A; ++i) {
-            if (P[i] <= 1) continue;
-            double r = weight[i] / P[i];
-            if (r < best_ratio) { best_ratio = r; best = i; }
-        }
-        if (best < 0) break;
-        P[best] -= 1;
-        --used;
+        if (worst < 0) break;
+        const int cur = span(worst, P[worst]);
+        if (cur <= 1) break;                                   // one tile per CTA already
+        const int need = (tiles[worst] + (cur - 1) - 1) / (cur - 1);   // fewest CTAs with span cur - 1
+        if (used + (need - P[worst]) > G) break;
+        used += need - P[worst];
+        P[worst] = need;
     }
     return P;
 }
