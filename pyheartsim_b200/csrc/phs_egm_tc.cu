@@ -22,7 +22,8 @@
 // with 4 stages of BK 32, 128 x 128 with 6 stages of BK 32.  The 256-wide tiles
 // read 0.75 of the operand bytes per FLOP of the 128-wide ones (the operands
 // stream from L2); the BK-32 rings keep more, smaller stages in flight ahead of
-// the MMAs.  phs_egm_contract_bf16x3 uses kTcDefaultConfig;
+// the MMAs (measured slower: their 64-byte TMA rows move less per request).
+// phs_egm_contract_bf16x3 uses kTcDefaultConfig;
 // phs_egm_contract_bf16x3_cfg takes a configuration (the autotuner's choice).
 // Split-K partials are summed in split order by a second kernel.
 //
@@ -364,7 +365,9 @@ constexpr TcConfig tc_config() {
 const TcConfig kTcConfigs[] = {tc_config<128, 64, 3>(), tc_config<256, 64, 2>(), tc_config<256, 32, 4>(),
                                tc_config<128, 32, 6>()};
 constexpr int kTcNumConfigs = 4;
-constexpr int kTcDefaultConfig = 0;
+// 128 x 256 tiles, 2 stages of BK 64: the fastest at 1000 x 519,533 x 2048
+// (5.09 ms against 5.78 ms for 128 x 128; the BK-32 rings took 8.7 and 10.7 ms).
+constexpr int kTcDefaultConfig = 1;
 
 // Columns of the split-K partial tiles: n_e_pad rounded up to the tile width.
 int64_t partial_cols(int64_t E_pad, int bn) { return (E_pad + bn - 1) / bn * bn; }

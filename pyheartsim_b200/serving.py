@@ -10,10 +10,10 @@ between launches,
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
 * retires instances that reached their last step: gathers the whole 1 kHz Vm
-  history into the caller's voxel order on the device, frees the instance and
-  copies the history to the host on a worker thread while the engine runs on
-  (a request's latency ends when its history is on the host; the device copy
-  counts against the budget until then);
+  history into the caller's voxel order on the device, copies it to the host
+  (a request's latency ends when its history is there) and frees the
+  instance.  (Copying on worker threads while the engine ran on was measured
+  slower: large pageable copies stall the main thread's launches.);
 * re-splits CTAs over the running instances by measured cost every
   ``rebalance_every`` launches (the device phase timers run only in the launch
   before each re-split).
@@ -168,40 +168,8 @@ class Server:
         t0 = time.perf_counter()
         nxt = 0
         work = 0.0
-        # retired histories go to the host on worker threads while the engine
-        # keeps running: gathered into caller order on the device (side
-        # stream), the instance removed, the device copy counted against the
-        # budget until the host has it
         dev_dl = hasattr(self.engine, "history_device")
-        if dev_dl:
-            import torch
-            dl_stream = torch.cuda.Stream()
-            dl_pool = ThreadPoolExecutor(max_workers=2)
-        downloads = []
-
-        def fetch(r, t):
-            with torch.cuda.stream(dl_stream):
-                hist = t.cpu().numpy()
-            r.history_bytes = hist.nbytes
-            r.history = hist if keep_history else None
-            r.done_s = time.perf_counter() - t0
-
-        def finish_downloads(block=False):
-            nonlocal downloads
-            keep = []
-            for r, fut, hold in downloads:
-                if block or fut.done():
-                    fut.result()
-                    self.used -= hold
-                    done.append(r)
-                    if log:
-                        log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
-                else:
-                    keep.append((r, fut, hold))
-            downloads = keep
-
-        while nxt < len(reqs) or queue or active or downloads:
-            finish_downloads()
+        while nxt < len(reqs) or queue or active:
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival_s * time_scale <= now:
                 queue.append(reqs[nxt])
@@ -229,8 +197,6 @@ class Server:
             if not active:
                 if nxt < len(reqs):
                     time.sleep(max(0.0, min(0.05, reqs[nxt].arrival_s * time_scale - now)))
-                elif downloads:
-                    time.sleep(0.002)
                 continue
             # phase timers only for the launch whose costs the next re-split uses
             due = (self.launches + 1) % self.rebalance_every == 0
@@ -247,15 +213,8 @@ class Server:
                     r = active.pop(slot)
                     r.status = info["status"]
                     work += float(r.inst.n_voxel) * info["step"]
-                    if dev_dl:
-                        t = self.engine.history_device(slot, stream=dl_stream)
-                        dl_stream.synchronize()           # the gather has read the engine's rows
-                        self.engine.remove(slot)
-                        hold = t.numel() * t.element_size()
-                        self.used += hold - r.fp
-                        downloads.append((r, dl_pool.submit(fetch, r, t), hold))
-                        continue
-                    hist = self.engine.history(slot)           # the whole 1 kHz Vm history, to the host
+                    # the whole 1 kHz Vm history, to the host (caller order made on the device)
+                    hist = self.engine.history_device(slot).cpu().numpy() if dev_dl else self.engine.history(slot)
                     r.history_bytes = hist.nbytes
                     r.history = hist if keep_history else None
                     r.done_s = time.perf_counter() - t0
@@ -264,9 +223,6 @@ class Server:
                     done.append(r)
                     if log:
                         log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
-        finish_downloads(block=True)
-        if dev_dl:
-            dl_pool.shutdown()
         makespan = time.perf_counter() - t0
         return done, {"makespan_s": makespan, "voxel_steps": work, "launches": self.launches}
 
