@@ -163,6 +163,10 @@ int64_t phs_engine_launch_count(phs_engine* eng);
                                     many as the grid holds).  Each wave is one launch over the whole
                                     grid for the same steps, one wave after another, so a wave's
                                     instances have the L2 to themselves                             */
+#define PHS_CFG_GROUP_SUMS 7  /* FP64 engines: 1 (default) combines the per-tile partial sums of
+                                 every reduction in fixed groups of 8 consecutive tiles before the
+                                 leader CTA sums the groups; 0: the leader sums every tile.  The
+                                 order is fixed either way (results do not depend on team size) */
 int phs_engine_config(phs_engine* eng, int key, int64_t value);
 /* Compiled step-kernel variants of a precision: count, and per variant the
  * minimum CTAs per SM it was compiled for and its register count (arrays of at

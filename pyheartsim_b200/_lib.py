@@ -35,6 +35,7 @@ CFG_PROFILE = 3
 CFG_TEST_TEAM_OVERCOUNT = 4
 CFG_AUTO_BALANCE = 5
 CFG_WAVE_INSTANCES = 6
+CFG_GROUP_SUMS = 7
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
                  "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas")
 

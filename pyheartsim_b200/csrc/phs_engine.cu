@@ -366,6 +366,7 @@ constexpr bool kWarpParts = sizeof(T) == 4;
 // by whichever CTA finishes a group's last tile, so the leader reads one
 // partial per group (GMRES(50) reduces up to 51 slots per barrier).
 constexpr int kGroupTiles = 8;
+constexpr int kMaxGroupWalk = 32;   // tiles a CTA counts in per pass
 
 // ------------------------------------------------------------------ the kernel
 // EDGE: the launch carries anisotropic instances (edge cross terms); the
@@ -398,8 +399,9 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
 
     const long long N = I.n;
     const int ps = I.ps;
-    const int nparts = kWarpParts<T> ? I.n_tiles * kWarps : I.n_groups;
-    const double* psum = kWarpParts<T> ? I.part : I.gpart;   // what the leader sums
+    const bool grouped = !kWarpParts<T> && I.gpart != nullptr;
+    const int nparts = kWarpParts<T> ? I.n_tiles * kWarps : (grouped ? I.n_groups : I.n_tiles);
+    const double* psum = grouped ? I.gpart : I.part;   // what the leader sums
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     Scalars* sc = I.sc;
@@ -440,7 +442,6 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             if (lane == 0) red[red_buf][warp][slot] = v;
         }
     };
-    __shared__ int sh_glast;
     auto tile_done = [&](int tile, int nslot) {
         if constexpr (!kWarpParts<T>) {
             __syncthreads();
@@ -451,27 +452,45 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 I.part[(size_t)tile * ps + t] = a;
             }
             red_buf ^= 1;
-            // the CTA that completes a group of tiles sums the group, tiles in order
-            const int g = tile / kGroupTiles;
-            const int t0 = g * kGroupTiles;
-            const int t1 = min(t0 + kGroupTiles, I.n_tiles);
-            __threadfence();
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                const unsigned int prev = atomicAdd(I.gcnt + g, 1u);
-                sh_glast = (prev == (unsigned int)(t1 - t0 - 1));
-            }
-            __syncthreads();
-            if (sh_glast) {
-                __threadfence();
-                for (int t = threadIdx.x; t < nslot; t += kThreads) {
-                    double a = 0.0;
-                    for (int q = t0; q < t1; ++q) a += __ldcg(I.part + (size_t)q * ps + t);
-                    I.gpart[(size_t)g * ps + t] = a;
+        }
+    };
+    // After a CTA's tiles of a phase (FP64 with group sums): one fence, then
+    // the CTA counts its tiles in at their groups; the CTA whose tile completes
+    // a group sums that group's tiles in order.  Every tile of a group arrives
+    // once per phase and the next phase's arrivals follow the team barrier, so
+    // the completing CTA resets the counter.
+    __shared__ int sh_glast[kMaxGroupWalk];
+    __shared__ int sh_nlast;
+    auto groups_done = [&](int nslot) {
+        if constexpr (!kWarpParts<T>) {
+            if (I.gpart == nullptr) return;
+            for (int base = rank; base < I.n_tiles; base += kMaxGroupWalk * P) {
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    __threadfence();
+                    int nl = 0;
+                    for (int q = 0; q < kMaxGroupWalk; ++q) {
+                        const int tile = base + q * P;
+                        if (tile >= I.n_tiles) break;
+                        const int g = tile / kGroupTiles;
+                        const int gsz = min(kGroupTiles, I.n_tiles - g * kGroupTiles);
+                        if (atomicAdd(I.gcnt + g, 1u) == (unsigned int)(gsz - 1)) sh_glast[nl++] = g;
+                    }
+                    sh_nlast = nl;
+                    __threadfence();
                 }
-                // every tile of the group has arrived in this phase; the next
-                // phase's arrivals come after the team barrier
-                if (threadIdx.x == 0) I.gcnt[g] = 0u;
+                __syncthreads();
+                for (int q = 0; q < sh_nlast; ++q) {
+                    const int g = sh_glast[q];
+                    const int t0 = g * kGroupTiles;
+                    const int t1 = min(t0 + kGroupTiles, I.n_tiles);
+                    for (int t = threadIdx.x; t < nslot; t += kThreads) {
+                        double a = 0.0;
+                        for (int u = t0; u < t1; ++u) a += __ldcg(I.part + (size_t)u * ps + t);
+                        I.gpart[(size_t)g * ps + t] = a;
+                    }
+                    if (threadIdx.x == 0) I.gcnt[g] = 0u;
+                }
             }
         }
     };
@@ -906,6 +925,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             put(tile, 1, ar);
             tile_done(tile, 2);
         }
+        groups_done(2);
         mark(PF_RHS);
         if (!team_sync(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
         int act = read_action();
@@ -975,6 +995,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                         }
                         tile_done(tile, j + 1);
                     }
+                    groups_done(j + 1);
                     mark(PF_A);
                     if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_dots(j); })) { aborted = true; break; }
                     load_shc(j + 1);
@@ -1021,6 +1042,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                         put(tile, 0, a2);
                         tile_done(tile, 1);
                     }
+                    groups_done(1);
                     mark(PF_C);
                     if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_norm(j); })) { aborted = true; break; }
                     act = read_action();
@@ -1116,6 +1138,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     put(tile, 0, a2);
                     tile_done(tile, 1);
                 }
+                groups_done(1);
                 mark(PF_CHECK);
                 if (!team_sync(I.sync, P, abort_word, ctl, leader_check)) { aborted = true; break; }
                 act = read_action();
@@ -1339,6 +1362,7 @@ struct phs_engine {
     bool test_overcount = false;  // test hook: first team waits for one CTA too many
     int default_cps = 0;     // CTAs per SM when advance() is given 0 (0: occupancy limit)
     int wave_instances = 0;  // instances per launch wave (0: as many as the grid holds)
+    bool group_sums = true;  // FP64: partial sums combined in groups of tiles before the leader
 };
 
 namespace {
@@ -1562,7 +1586,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
 }
 
 template <typename T>
-InstDev<T> make_dev(const InstHost& h) {
+InstDev<T> make_dev(const InstHost& h, bool group_sums) {
     InstDev<T> I{};
     I.nb = (const int32_t*)h.nb;
     I.coef = (const T*)h.coef;
@@ -1584,7 +1608,7 @@ InstDev<T> make_dev(const InstHost& h) {
     I.hist_h = (T*)h.hist_h;
     I.lat = h.lat;
     I.part = h.part;
-    I.gpart = h.gpart;
+    I.gpart = group_sums ? h.gpart : nullptr;
     I.gcnt = h.gcnt;
     I.n_groups = h.n_groups;
     I.sc = h.sc;
@@ -1701,7 +1725,7 @@ int build_plan(phs_engine* e, int cps, bool edge) {
     if (act.empty()) return PHS_OK;
     std::vector<InstDev<T>> descs;
     descs.reserve(act.size());
-    for (int i : act) descs.push_back(make_dev<T>(e->inst[i]));
+    for (int i : act) descs.push_back(make_dev<T>(e->inst[i], e->group_sums));
     size_t bytes = descs.size() * sizeof(InstDev<T>);
     if (bytes > e->d_desc_bytes) {
         if (e->d_desc) cudaFree(e->d_desc);
@@ -2076,6 +2100,12 @@ int phs_engine_config(phs_engine* e, int key, int64_t value) {
             // the caller's setting wins over the automatic balancing's
             e->auto_prof = false;
             return set_profile(e, value != 0);
+        case PHS_CFG_GROUP_SUMS:
+            if (e->group_sums != (value != 0)) {
+                e->group_sums = value != 0;
+                e->dirty = true;
+            }
+            return PHS_OK;
         case PHS_CFG_WAVE_INSTANCES:
             if (value < 0 || value > (1 << 20)) return PHS_ERR_BAD_ARG;
             if (e->wave_instances != (int)value) {
