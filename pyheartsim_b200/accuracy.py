@@ -62,20 +62,32 @@ def compare_activations(ref, test, max_activations=MAX_ACTIVATIONS):
     Returns the first-activation error (max over voxels activated in both runs,
     and the count activated in only one), and per re-activation index i the
     voxels with at least i+1 activations in both, their max |dLAT|, and the
-    voxels with i+1 activations in one run only."""
+    voxels with i+1 activations in one run only.  ``nearest_*`` pair each
+    reference activation with the test run's nearest crossing of the same
+    voxel instead of the one with the same count."""
     cr, ct = ref["counts"], test["counts"]
     tr, tt = ref["times"].astype(np.int64), test["times"].astype(np.int64)
     out = {"voxels": int(cr.size), "activation_count_equal_frac": float(np.mean(cr == ct)),
            "max_activations_ref": int(cr.max()), "max_activations_test": int(ct.max())}
     per = []
+    valid_t = tt >= 0
     for i in range(min(max_activations, int(max(cr.max(), ct.max())))):
         both = (cr > i) & (ct > i)
         one = int(((cr > i) != (ct > i)).sum())
         d = np.abs(tr[both, i] - tt[both, i])
+        # the same activation found by time instead of by count: the test
+        # run's nearest crossing of that voxel (an extra or missing crossing
+        # elsewhere in the sequence does not shift the pairing)
+        has = cr > i
+        near = np.where(valid_t[has], np.abs(tt[has] - tr[has, i][:, None]), np.iinfo(np.int64).max).min(axis=1)
+        near = near[near < np.iinfo(np.int64).max]
         per.append({"index": i, "voxels_both": int(both.sum()), "voxels_one_run_only": one,
                     "max_dlat_steps": int(d.max()) if d.size else None,
                     "p99_dlat_steps": float(np.percentile(d, 99)) if d.size else None,
-                    "frac_within_1_step": float(np.mean(d <= 1)) if d.size else None})
+                    "frac_within_1_step": float(np.mean(d <= 1)) if d.size else None,
+                    "nearest_max_dlat_steps": int(near.max()) if near.size else None,
+                    "nearest_p99_dlat_steps": float(np.percentile(near, 99)) if near.size else None,
+                    "nearest_frac_within_1_step": float(np.mean(near <= 1)) if near.size else None})
     out["first"] = per[0] if per else None
     out["reactivations"] = per[1:]
     return out
