@@ -812,21 +812,9 @@ def egm_leg(args, dev, history=None):
         _lib.check(L.phs_egm_contract_bf16x3_cfg(T, n_e, Tp, Ep, Kp, p(vh), p(vl), p(mh), p(ml), p(out), p(work),
                                                  cfg, sp), "contract_bf16x3")
 
-    # tile configurations (the autotuner's choice): median of 3 timed calls each
-    cfg_ms = {}
-    for cfg in range(L.phs_egm_bf16x3_config_count()):
-        contract(cfg)           # warm-up
-        times = []
-        for _ in range(3):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            contract(cfg)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-        _lib.check(L.phs_egm_bf16x3_status(p(work), sp), "contract_bf16x3 status")
-        cfg_ms[cfg] = sorted(times)[1]
-    best = min(cfg_ms, key=cfg_ms.get)
+    # tile configuration from the autotuner (median of 3 timed calls each)
+    from pyheartsim_b200 import autotune
+    best, cfg_ms = autotune.tune_electrogram(T, n_e, Tp, Ep, Kp, vh, vl, mh, ml, out, work, stream=stream)
     contract(best)
     ev[4].record(stream)
     for _ in range(reps):
@@ -852,8 +840,7 @@ def egm_leg(args, dev, history=None):
                        "history": "S1-S2 run of the FP32 engine (Mitchell-Schaeffer, S2 at 250 ms)",
                        "simulation_s": sim_s},
             "bf16x3_ms": ms_bf, "tile_config": int(best),
-            "tile_config_ms": {["128x128 BK64 x3", "128x256 BK64 x2", "128x256 BK32 x4", "128x128 BK32 x6"][k]: v
-                               for k, v in cfg_ms.items()},
+            "tile_config_ms": {autotune.EGM_TILE_NAMES[k]: v for k, v in cfg_ms.items()},
             "useful_tflops": flops / (ms_bf / 1e3) / 1e12, "executed_tflops": tf_exec,
             "tensor_frac": tf_exec / pk["bf16_tflops"], "peak_tflops": pk["bf16_tflops"], "peak_source": pk_src,
             "fp64_contract_ms": ms_f64, "fp64_tflops": flops / (ms_f64 / 1e3) / 1e12,

@@ -1,4 +1,4 @@
-"""Autotuner of the step kernel.
+"""Autotuners of the step kernel and of the electrogram contraction.
 
 Times every compiled step-kernel variant (voxels per thread, i.e. the tile
 length of 256 x VPT voxels, and register budget) at every feasible
@@ -12,6 +12,9 @@ Results are cached per GPU name and workload bucket (precision, total voxels
 rounded to a power of two, instance count): in the process, and in a JSON file
 (``PHS_AUTOTUNE_CACHE``, default ``~/.cache/pyheartsim_b200/autotune.json``)
 so later processes on the same machine start from the same choice.
+
+:func:`tune_electrogram` picks the tile configuration (output tile 128 x 128 or
+128 x 256, K stage width and depth) of the BF16x3 electrogram contraction.
 """
 import json
 import math
@@ -98,3 +101,46 @@ def tune(engine, steps=10, stream=None, cps_options=None, repeats=5, use_file=Tr
         _store_file(key, _CACHE[key])
     engine.configure(variant=best["variant"], ctas_per_sm=best["ctas_per_sm"])
     return {"cached": False, "best": (best["variant"], best["ctas_per_sm"]), "table": table}
+
+
+_EGM_CACHE = {}
+EGM_TILE_NAMES = ("128x128 BK64 x3", "128x256 BK64 x2", "128x256 BK32 x4", "128x128 BK32 x6")
+
+
+def tune_electrogram(T, n_e, T_pad, E_pad, K_pad, vh, vl, mh, ml, out, work, stream=None, repeats=3):
+    """Pick the tcgen05 tile configuration of the BF16x3 electrogram contraction
+    (``phs_egm_contract_bf16x3_cfg``) for this shape: every configuration is
+    run once to warm up, then timed ``repeats`` times (CUDA events on the
+    stream) and ranked by the median.  The operands are device tensors (the
+    split V and M), ``out`` the (T, n_e) FP32 result and ``work`` the workspace.
+    Cached per GPU name and padded shape.  Returns (best config, {config:
+    median ms})."""
+    import ctypes
+    key = (torch.cuda.get_device_name(), int(T_pad), int(E_pad), int(K_pad))
+    if key in _EGM_CACHE:
+        return _EGM_CACHE[key]
+    L = _lib.lib()
+    stream = stream or torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def run(cfg):
+        _lib.check(L.phs_egm_contract_bf16x3_cfg(T, n_e, T_pad, E_pad, K_pad, p(vh), p(vl), p(mh), p(ml), p(out),
+                                                 p(work), cfg, sp), "phs_egm_contract_bf16x3_cfg")
+
+    ms = {}
+    for cfg in range(L.phs_egm_bf16x3_config_count()):
+        run(cfg)
+        times = []
+        for _ in range(max(1, repeats)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(cfg)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        _lib.check(L.phs_egm_bf16x3_status(p(work), sp), "phs_egm_bf16x3_status")
+        ms[cfg] = sorted(times)[len(times) // 2]
+    best = min(ms, key=ms.get)
+    _EGM_CACHE[key] = (best, ms)
+    return best, ms
