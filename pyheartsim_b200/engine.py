@@ -117,6 +117,47 @@ class BatchedEngine:
                 out = src.index_select(1, inv)
         return out
 
+    def history_host(self, slot, s0=0, count=None, stage_bytes=128 << 20):
+        """The instance's Vm history (count, n) in the caller's voxel order as a
+        numpy array, fast: gathered into caller order on the device, copied to
+        the host through two reused pinned staging buffers of ``stage_bytes``
+        (each chunk's device-to-host copy overlaps the host copy of the one
+        before).  Same values as :meth:`history`."""
+        import torch
+        t = self.history_device(slot, s0, count)
+        rows, n = t.shape
+        out = np.empty((rows, n), dtype=_lib.np_dtype(self.precision))
+        if rows == 0:
+            return out
+        dev = t.device
+        per = max(1, int(stage_bytes // max(1, n * t.element_size())))
+        st = getattr(self, "_stage", None)
+        if st is None or st[0].numel() < per * n or st[0].dtype != t.dtype:
+            st = [torch.empty(per * n, dtype=t.dtype, pin_memory=True) for _ in range(2)]
+            self._stage = st
+        stream = torch.cuda.Stream(dev)
+        events = [None, None]
+        prev = None
+        with torch.cuda.stream(stream):
+            for k, a in enumerate(range(0, rows, per)):
+                b = min(rows, a + per)
+                buf = st[k % 2]
+                if events[k % 2] is not None:
+                    events[k % 2].synchronize()          # its previous chunk has been copied out below
+                buf[:(b - a) * n].view(b - a, n).copy_(t[a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                if prev is not None:
+                    pa, pb, pbuf, pev = prev
+                    pev.synchronize()
+                    np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
+                prev = (a, b, buf, ev)
+                events[k % 2] = ev
+            pa, pb, pbuf, pev = prev
+            pev.synchronize()
+            np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
+        return out
+
     def activation_times(self, slot, max_per_voxel=16, threshold=0.5, stream=None):
         """Every upward crossing of ``threshold`` by Vm in the instance's device
         history (``phs_activation_times``): ``(times, counts)`` in the caller's

@@ -5,7 +5,9 @@ over time.  The server keeps one FP32 :class:`BatchedEngine` on the GPU and,
 between launches,
 
 * admits waiting requests in arrival order while their device footprint fits
-  the HBM budget (FIFO: the head of the queue is never overtaken);
+  the HBM budget and fewer than ``max_active`` run (FIFO: the head of the
+  queue is never overtaken; a few hundred instances at once would leave each
+  one or two CTAs and spend the launch on team barriers);
 * advances every admitted instance by ``steps_per_launch`` steps in one
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
@@ -143,14 +145,18 @@ class _Inline:
 
 class Server:
     def __init__(self, hbm_budget_bytes, steps_per_launch=50, rebalance_every=8, build_threads=8, tol=1e-7,
-                 stream=None, engine=None, builder=None, footprint=None, device_build=False):
+                 stream=None, engine=None, builder=None, footprint=None, device_build=False, max_active=64):
         self.budget = int(hbm_budget_bytes)
+        self.max_active = int(max_active)
         self.S = int(steps_per_launch)
         self.rebalance_every = int(rebalance_every)
         self.tol = tol
         self.builder = builder or (lambda r: build(r, self.tol, device=device_build))
         self.footprint = footprint or footprint_bytes
-        self.engine = engine if engine is not None else BatchedEngine(_lib.PREC_F32)
+        if engine is None:
+            engine = BatchedEngine(_lib.PREC_F32)
+            engine.configure(auto_balance=False)      # the server re-splits the CTAs itself
+        self.engine = engine
         self.pool = ThreadPoolExecutor(max_workers=build_threads) if build_threads > 0 else _Inline()
         self.stream = stream
         self.used = 0
@@ -168,7 +174,7 @@ class Server:
         t0 = time.perf_counter()
         nxt = 0
         work = 0.0
-        dev_dl = hasattr(self.engine, "history_device")
+        dev_dl = hasattr(self.engine, "history_host")
         while nxt < len(reqs) or queue or active:
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival_s * time_scale <= now:
@@ -181,7 +187,7 @@ class Server:
                     break                                  # head still compiling; keep the GPU busy
                 inst = r.future.result()
                 fp = self.footprint(inst)
-                if active and self.used + fp > self.budget:
+                if active and (self.used + fp > self.budget or len(active) >= self.max_active):
                     break
                 queue.popleft()
                 r.inst = inst
@@ -214,7 +220,7 @@ class Server:
                     r.status = info["status"]
                     work += float(r.inst.n_voxel) * info["step"]
                     # the whole 1 kHz Vm history, to the host (caller order made on the device)
-                    hist = self.engine.history_device(slot).cpu().numpy() if dev_dl else self.engine.history(slot)
+                    hist = self.engine.history_host(slot) if dev_dl else self.engine.history(slot)
                     r.history_bytes = hist.nbytes
                     r.history = hist if keep_history else None
                     r.done_s = time.perf_counter() - t0
