@@ -1255,22 +1255,31 @@ using namespace phs;
 namespace {
 
 constexpr int kVptF32 = 4;
+constexpr int kVptF32Min = 2;    // the smallest voxels-per-thread of any FP32 variant
 constexpr int kVptF64 = 1;
 
-// Compiled step-kernel variants: same algorithm and tiling, different register
-// budgets (__launch_bounds__ minimum CTAs per SM).  The autotuner picks one.
-// Each exists without and with the anisotropic edge terms.
+// Compiled step-kernel variants: the same algorithm with different tile
+// lengths (voxels per thread; a tile is 256 x VPT consecutive voxels) and
+// register budgets (__launch_bounds__ minimum CTAs per SM).  The autotuner
+// picks one.  Each exists without and with the anisotropic edge terms.
 using StepFnF = void (*)(const InstDev<float>*, const int4*, long long, unsigned int*);
 using StepFnD = void (*)(const InstDev<double>*, const int4*, long long, unsigned int*);
 const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2, false>, step_kernel<float, kVptF32, 3, false>,
-                            step_kernel<float, kVptF32, 4, false>};
+                            step_kernel<float, kVptF32, 4, false>, step_kernel<float, 2, 4, false>,
+                            step_kernel<float, 2, 5, false>};
 const StepFnF kStepF32Edge[] = {step_kernel<float, kVptF32, 2, true>, step_kernel<float, kVptF32, 3, true>,
-                                step_kernel<float, kVptF32, 4, true>};
-const int kMinbF32[] = {2, 3, 4};
+                                step_kernel<float, kVptF32, 4, true>, step_kernel<float, 2, 4, true>,
+                                step_kernel<float, 2, 5, true>};
+const int kMinbF32[] = {2, 3, 4, 4, 5};
+const int kVptOfF32[] = {kVptF32, kVptF32, kVptF32, 2, 2};
 const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2, false>, step_kernel<double, kVptF64, 3, false>};
 const StepFnD kStepF64Edge[] = {step_kernel<double, kVptF64, 2, true>, step_kernel<double, kVptF64, 3, true>};
 const int kMinbF64[] = {2, 3};
-constexpr int kNumF32 = 3, kNumF64 = 2;
+constexpr int kNumF32 = 5, kNumF64 = 2;
+
+// Tiles of an instance of n voxels under a variant.
+int tiles_of(long long n, int vpt) { return (int)((n + (long long)kThreads * vpt - 1) / ((long long)kThreads * vpt)); }
+int vpt_of(int prec_bytes, int variant) { return prec_bytes == 8 ? kVptF64 : kVptOfF32[variant]; }
 // FP32: 64 registers, 4 CTAs/SM (the autotuner's pick on B200); FP64: 80
 // registers, 3 CTAs/SM (plain GMRES(50) on a 157k-voxel shell: 2.06 ms per
 // step against 2.46 ms with 128 registers and 2 CTAs/SM)
@@ -1465,7 +1474,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     h.used = true;
     h.d = *d;
     h.n = d->n_voxel;
-    const int vpt = sizeof(T) == 8 ? kVptF64 : kVptF32;
+    const int vpt = sizeof(T) == 8 ? kVptF64 : kVptF32Min;   // allocations cover every variant's tiles
     const long long tile = (long long)kThreads * vpt;
     h.n_tiles = (int)((h.n + tile - 1) / tile);
     h.m = (int)std::min<long long>(d->restart, h.n);
@@ -1589,7 +1598,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
 }
 
 template <typename T>
-InstDev<T> make_dev(const InstHost& h, bool group_sums) {
+InstDev<T> make_dev(const InstHost& h, bool group_sums, int vpt) {
     InstDev<T> I{};
     I.nb = (const int32_t*)h.nb;
     I.coef = (const T*)h.coef;
@@ -1613,7 +1622,7 @@ InstDev<T> make_dev(const InstHost& h, bool group_sums) {
     I.part = h.part;
     I.gpart = group_sums ? h.gpart : nullptr;
     I.gcnt = h.gcnt;
-    I.n_groups = h.n_groups;
+    I.n_groups = (tiles_of(h.n, vpt) + kGroupTiles - 1) / kGroupTiles;
     I.sc = h.sc;
     I.sync = h.sync;
     I.st = h.st;
@@ -1629,7 +1638,7 @@ InstDev<T> make_dev(const InstHost& h, bool group_sums) {
     I.n = h.n;
     I.n_steps = h.d.n_steps;
     I.tb_steps = h.d.tblock_steps;
-    I.n_tiles = h.n_tiles;
+    I.n_tiles = tiles_of(h.n, vpt);
     I.ps = h.m + 2;
     I.model = h.d.model;
     I.m = h.m;
@@ -1728,7 +1737,8 @@ int build_plan(phs_engine* e, int cps, bool edge) {
     if (act.empty()) return PHS_OK;
     std::vector<InstDev<T>> descs;
     descs.reserve(act.size());
-    for (int i : act) descs.push_back(make_dev<T>(e->inst[i], e->group_sums));
+    const int vpt = vpt_of((int)sizeof(T), variant_of<T>(e));
+    for (int i : act) descs.push_back(make_dev<T>(e->inst[i], e->group_sums, vpt));
     size_t bytes = descs.size() * sizeof(InstDev<T>);
     if (bytes > e->d_desc_bytes) {
         if (e->d_desc) cudaFree(e->d_desc);
@@ -1751,7 +1761,7 @@ int build_plan(phs_engine* e, int cps, bool edge) {
         for (size_t i = w0; i < w1; ++i) measured = measured && e->inst[act[i]].weight > 0.0;
         for (size_t i = w0; i < w1; ++i) {
             const InstHost& h = e->inst[act[i]];
-            tiles.push_back(h.n_tiles);
+            tiles.push_back(tiles_of(h.n, vpt));
             weight.push_back(measured ? h.weight : (double)h.n * (1.6 + h.kavg));
         }
         std::vector<int> P = team_sizes(tiles, weight, G);
@@ -2072,7 +2082,7 @@ int phs_step_variant_vpt(int precision, int32_t count, int32_t* vpt) {
     if (precision != PHS_PREC_F32 && precision != PHS_PREC_F64) return PHS_ERR_BAD_ARG;
     const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
     if (count < nv || !vpt) return PHS_ERR_BAD_ARG;
-    for (int v = 0; v < nv; ++v) vpt[v] = precision == PHS_PREC_F64 ? kVptF64 : kVptF32;
+    for (int v = 0; v < nv; ++v) vpt[v] = precision == PHS_PREC_F64 ? kVptF64 : kVptOfF32[v];
     return PHS_OK;
 }
 
