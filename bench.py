@@ -31,11 +31,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
 # DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, median of 24 full-size launches of this batch at 2.05
+# dram__bytes_write.sum of the two timed full-size launches of this batch, 2.71
 # Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md);
 # multiplied by the voxels and steps of one launch below.
-STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 232.4
-STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.05
+STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 267.0
+STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.71
 BALANCE_LAUNCHES = 10   # launches per team-balancing round in the pre-steps
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
 
