@@ -328,12 +328,14 @@ def run_b200(args):
 
 
 def step_kernel_name(tune):
-    """Template arguments of the step-kernel variant the timed launches used."""
+    """Template arguments (value type, voxels per thread, minimum CTAs per SM,
+    edge terms) of the step-kernel variant the timed launches used."""
     from pyheartsim_b200.engine import step_variants
     from pyheartsim_b200 import _lib
-    var = {v: minb for v, minb, _ in step_variants(_lib.PREC_F32)}
-    v = tune["best"][0] if tune is not None else None
-    return f"step_kernel<float,4,{var[v]},false>" if v in var else "step_kernel<float,4,default,false>"
+    var = {v: (minb, vpt) for v, minb, _, vpt in step_variants(_lib.PREC_F32, with_vpt=True)}
+    v = tune["best"][0] if tune is not None else 2
+    minb, vpt = var[v]
+    return f"step_kernel<float,{vpt},{minb},false>"
 
 
 def phase_profile(eng, slots, S, stream):

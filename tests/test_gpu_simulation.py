@@ -10,6 +10,8 @@ pytestmark = pytest.mark.gpu
 
 # plain FP64 form vs the reference's own FP64 run / the FP64 oracle
 PLAIN_ATOL = 1e-9
+# FP32 early-exit form vs the FP64 oracle, max |dVm| over the run's samples
+FAST_DVM = 1e-3
 
 
 @pytest.mark.parametrize("name", golden_cases.names())
@@ -48,7 +50,9 @@ def test_fast_fp32_lat_within_one_step(case, cuda_device):
     both = (lat >= 0) & (lato >= 0)
     assert np.array_equal(lat >= 0, lato >= 0)
     assert np.abs(lat[both].astype(np.int64) - lato[both]).max() <= 1
-    assert np.abs(u - uo).max() < 2e-2
+    # measured max |dVm| of these four cases: 2.2e-4 (sheet), 6.7e-6 (AP slab),
+    # 4.1e-5 and 3.5e-5 (shells); the bound is about five times the largest
+    assert np.abs(u - uo).max() < FAST_DVM
 
 
 def test_repeat_is_bit_identical(cuda_device):
