@@ -167,6 +167,12 @@ int64_t phs_engine_launch_count(phs_engine* eng);
                                  every reduction in fixed groups of 8 consecutive tiles before the
                                  leader CTA sums the groups; 0: the leader sums every tile.  The
                                  order is fixed either way (results do not depend on team size) */
+#define PHS_CFG_COMPACT_NB 9  /* 1 (default): an instance whose present neighbours of slots 0 and 1
+                                 are n+1 and n-1 (the +-x ones in the lattice row order) and whose
+                                 other slots' offsets fit int16 around a base per 512-voxel block
+                                 has a compact table (8 bytes per voxel instead of 24), read by the
+                                 variants of phs_step_variant_layout; same indices, same results.
+                                 0: every instance reads the int32 table                       */
 int phs_engine_config(phs_engine* eng, int key, int64_t value);
 /* Compiled step-kernel variants of a precision: count, and per variant the
  * minimum CTAs per SM it was compiled for and its register count (arrays of at
@@ -187,6 +193,9 @@ int phs_engine_rebalance(phs_engine* eng);
  * [9] final copy, [10] RHS pass 1 (reaction); [11] steps and
  * [12] Arnoldi iterations counted; [13] CTAs in the team at the last launch.   */
 int phs_instance_profile(phs_engine* eng, int slot, uint64_t* out16);
+/* Bytes per voxel of the neighbour table the instance's compact-table variants
+ * read: 8 (compact form, PHS_CFG_COMPACT_NB) or 24 (int32 table).              */
+int phs_instance_table_bytes(phs_engine* eng, int slot, int32_t* bytes_per_voxel);
 
 /* ------------------------------------------- one-shot drop-in (host buffers)
  * Runs a whole instance: upload, all steps, download.  Replaces

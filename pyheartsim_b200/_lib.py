@@ -36,6 +36,7 @@ CFG_TEST_TEAM_OVERCOUNT = 4
 CFG_AUTO_BALANCE = 5
 CFG_WAVE_INSTANCES = 6
 CFG_GROUP_SUMS = 7
+CFG_COMPACT_NB = 9
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
                  "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas")
 
@@ -157,6 +158,7 @@ SIGNATURES = {
     "phs_step_variant_vpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, c_int32_p]),
     "phs_instance_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "phs_engine_rebalance": (ctypes.c_int, [ctypes.c_void_p]),
+    "phs_instance_table_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int32_p]),
     "phs_simulate": (ctypes.c_int, [ctypes.POINTER(InstanceDesc), ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                     c_int32_p, c_int32_p, ctypes.POINTER(InstanceInfo)]),
     "phs_egm_leadfield_f64": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,

@@ -10,6 +10,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kMaxRestart = 50;            // GMRES(m) restart bound (reference uses m = 50)
 constexpr int kSlots = kMaxRestart + 2;    // FP64 partial sums per tile
 constexpr int kPhaseScalars = 4;
+constexpr int kPadVoxels = 1024;           // per-voxel engine arrays are padded to a multiple of this
 
 // Record a CUDA error message (host side); defined in phs_capi.cu.
 void set_last_error(const char* where, cudaError_t e);

@@ -27,6 +27,7 @@
 // size, so an instance gives bit-identical results alone and in a batch.
 #include <cuda_runtime.h>
 #include <cuda/atomic>
+#include <climits>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -95,6 +96,8 @@ struct InstState {
 template <typename T>
 struct InstDev {
     const int32_t* nb;      // [n*6]
+    const int16_t* nbr;     // [ldv*4] compact neighbour table (decode_nb), or nullptr
+    const int32_t* nbase;   // [ldv/512*4] its base offsets per 512-voxel block
     const T* coef;          // [n*6], or nullptr when every row is isotropic (cw, m6)
     const T* cw;            // [n] common coefficient of row n (isotropic rows)
     const uint8_t* m6;      // [n] neighbour presence bits of row n (isotropic rows)
@@ -124,6 +127,7 @@ struct InstDev {
     T dt, half_dt, jmag;
     double tol, atol;
     long long n;
+    long long ldv;          // padded voxel count (multiple of kPadVoxels): stride of V, length of per-voxel arrays
     long long n_steps;
     long long tb_steps;
     int n_tiles;
@@ -298,6 +302,22 @@ __device__ __forceinline__ void load_coef(const double* cf, long long n, double 
     const double2* p = reinterpret_cast<const double2*>(cf + 6 * n);
     double2 a = __ldg(p), b = __ldg(p + 1), d = __ldg(p + 2);
     c[0] = a.x; c[1] = a.y; c[2] = b.x; c[3] = b.y; c[4] = d.x; c[5] = d.y;
+}
+
+// Compact neighbour table.  In the row order of a lattice (x fastest) the
+// present +x and -x neighbours of voxel n are n + 1 and n - 1 (slots 0 and 1
+// of the reference's column order), and the other four slots hold offsets that
+// change slowly along the rows: base[r] of the voxel's 512-voxel block plus the
+// voxel's int16 residual r (slots 2..5).  Exact for every present neighbour
+// (checked when the table is built); absent ones decode to unused values.
+__device__ __forceinline__ void decode_nb(short4 r, int4 b, long long n, int32_t (&q)[6]) {
+    const int32_t nn = (int32_t)n;
+    q[0] = nn + 1;
+    q[1] = nn - 1;
+    q[2] = nn + b.x + r.x;
+    q[3] = nn + b.y + r.y;
+    q[4] = nn + b.z + r.z;
+    q[5] = nn + b.w + r.w;
 }
 
 // Coefficients of row n: one common value and a presence mask for isotropic
@@ -772,7 +792,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     T* Vb = I.V;
-    const size_t ldV = (size_t)N;
+    const size_t ldV = (size_t)I.ldv;
 
     // End-of-step work of voxel n whose new state un is known (the state after
     // step done_step): its sample into history slot `slot` (-1: none), its
@@ -793,7 +813,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         T us, hs;
         rk4(I.model, un, hn, J, p, I.dt, us, hs);
         hdst[n] = hs;
-        Vb[(size_t)N + n] = us;
+        Vb[ldV + n] = us;
     };
 
     // acc[v] += sum_{i < cnt} coef[i] * Vb[i][n_v], loads issued kChunk vectors at a time
@@ -1296,9 +1316,12 @@ struct InstHost {
     bool finished = false;
     phs_instance_desc d{};
     long long n = 0;
+    long long ldv = 0;           // padded voxel count: length of every per-voxel array
     int n_tiles = 0;
     int m = 0;
     void* nb = nullptr;
+    int16_t* nbr = nullptr;      // compact neighbour table, or nullptr
+    int32_t* nbase = nullptr;
     void* coef = nullptr;
     void* cw = nullptr;
     void* m6 = nullptr;
@@ -1335,7 +1358,7 @@ struct InstHost {
 };
 
 void free_inst(InstHost& h) {
-    void* ptrs[] = {h.nb, h.coef, h.cw, h.m6, h.enb, h.ecf, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
+    void* ptrs[] = {h.nb, h.nbr, h.nbase, h.coef, h.cw, h.m6, h.enb, h.ecf, h.dx, h.vflags, h.vparams, h.stim, h.u, h.h0, h.h1, h.x, h.b, h.V,
                     h.hist_u, h.hist_h, h.lat, h.part, h.gpart, h.gcnt, h.sc, h.sync, h.st, h.prof};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1375,6 +1398,7 @@ struct phs_engine {
     int default_cps = 0;     // CTAs per SM when advance() is given 0 (0: occupancy limit)
     int wave_instances = 0;  // instances per launch wave (0: as many as the grid holds)
     bool group_sums = true;  // FP64: partial sums combined in groups of tiles before the leader
+    bool compact_nb = true;  // instances read the compact neighbour table when they have one
 };
 
 namespace {
@@ -1413,10 +1437,102 @@ __global__ void check_tables(long long n, const int32_t* nb, const T* coef, cons
     }
 }
 
-// Copy n doubles (host, or device when on_device) into a new array of T.
+// ---- compact neighbour table (decode_nb)
+// Whether slot k of row v has a neighbour the operator reads: its coefficient
+// is nonzero, the test lap_row makes.
 template <typename T>
-int upload_converted(void** dst, const double* src, long long n, bool on_device = false) {
-    PHS_CUDA_TRY(cudaMalloc(dst, (size_t)n * sizeof(T)));
+__device__ __forceinline__ bool nb_present(const T* coef, const T* cw, const uint8_t* m6, long long v, int k) {
+    if (cw) return ((m6[v] >> k) & 1u) && cw[v] != T(0);
+    return coef[6 * v + k] != T(0);
+}
+
+// flags[k] bit 0: some present neighbour of slot k is not n + 1; bit 1: not n - 1.
+template <typename T>
+__global__ void nb_slot_kinds(long long n, const int32_t* nb, const T* coef, const T* cw, const uint8_t* m6,
+                              unsigned int* flags) {
+    unsigned int f[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        for (int k = 0; k < 6; ++k) {
+            if (!nb_present(coef, cw, m6, v, k)) continue;
+            const long long dq = (long long)nb[6 * v + k] - v;
+            f[k] |= (dq != 1 ? 1u : 0u) | (dq != -1 ? 2u : 0u);
+        }
+    }
+    for (int k = 0; k < 6; ++k) {
+        unsigned int a = f[k];
+        for (int o = 16; o > 0; o >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, o);
+        if ((threadIdx.x & 31) == 0 && a) atomicOr(flags + k, a);
+    }
+}
+
+// One CTA of 256 threads per 512-voxel block: for slots 2..5 the base offset
+// (middle of the block's range over present neighbours) and the int16
+// residuals; *fail set when a block's range does not fit.  Voxels past n
+// (padding) get zeros.
+template <typename T>
+__global__ void nb_compact(long long n, const int32_t* nb, const T* coef, const T* cw, const uint8_t* m6,
+                           int16_t* nbr, int32_t* nbase, unsigned int* fail) {
+    __shared__ long long lo[8][4], hi[8][4];
+    __shared__ int32_t base[4];
+    const long long v0 = (long long)blockIdx.x * 512;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long mn[4], mx[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) { mn[r] = LLONG_MAX; mx[r] = LLONG_MIN; }
+    for (int h = 0; h < 2; ++h) {
+        const long long v = v0 + h * 256 + threadIdx.x;
+        if (v >= n) continue;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (!nb_present(coef, cw, m6, v, r + 2)) continue;
+            const long long dq = (long long)nb[6 * v + r + 2] - v;
+            mn[r] = min(mn[r], dq);
+            mx[r] = max(mx[r], dq);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[r] = min(mn[r], (long long)__shfl_xor_sync(0xffffffffu, mn[r], o));
+            mx[r] = max(mx[r], (long long)__shfl_xor_sync(0xffffffffu, mx[r], o));
+        }
+        if (lane == 0) { lo[w][r] = mn[r]; hi[w][r] = mx[r]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int r = threadIdx.x;
+        long long a = LLONG_MAX, b = LLONG_MIN;
+        for (int q = 0; q < 8; ++q) { a = min(a, lo[q][r]); b = max(b, hi[q][r]); }
+        long long bs = 0;
+        if (a <= b) {
+            bs = a + (b - a) / 2;
+            if (b - bs > 32767 || a - bs < -32768 || bs > INT_MAX / 2 || bs < INT_MIN / 2) atomicOr(fail, 1u);
+        }
+        base[r] = (int32_t)bs;
+        nbase[blockIdx.x * 4 + r] = (int32_t)bs;
+    }
+    __syncthreads();
+    for (int h = 0; h < 2; ++h) {
+        const long long v = v0 + h * 256 + threadIdx.x;
+        long long d[4] = {0, 0, 0, 0};
+        if (v < n) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (nb_present(coef, cw, m6, v, r + 2)) d[r] = (long long)nb[6 * v + r + 2] - v - base[r];
+        }
+        short res[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) res[r] = (short)max(-32768ll, min(32767ll, d[r]));
+        reinterpret_cast<short4*>(nbr)[v] = make_short4(res[0], res[1], res[2], res[3]);
+    }
+}
+
+// Copy n doubles (host, or device when on_device) into a new array of T of
+// alloc_n >= n elements (the tail is zero).
+template <typename T>
+int upload_converted(void** dst, const double* src, long long n, bool on_device, long long alloc_n) {
+    PHS_CUDA_TRY(cudaMalloc(dst, (size_t)alloc_n * sizeof(T)));
+    if (alloc_n > n) PHS_CUDA_TRY(cudaMemset((char*)*dst + (size_t)n * sizeof(T), 0, (size_t)(alloc_n - n) * sizeof(T)));
     if (sizeof(T) == 8) {
         PHS_CUDA_TRY(cudaMemcpy(*dst, src, (size_t)n * 8, cudaMemcpyDefault));
         return PHS_OK;
@@ -1466,6 +1582,47 @@ int validate_desc(const phs_instance_desc* d) {
     return PHS_OK;
 }
 
+// Build the compact neighbour table (decode_nb) of an instance whose tables
+// are on the device (h.nb with the coefficients).  Leaves h.nbr null when a
+// present neighbour of slot 0 is not n + 1, one of slot 1 not n - 1, or a
+// block's offsets of another slot do not fit int16.
+template <typename T>
+int build_compact_nb(InstHost& h) {
+    const long long n = h.n;
+    unsigned int* d_w = nullptr;
+    PHS_CUDA_TRY(cudaMalloc((void**)&d_w, 8 * sizeof(unsigned int)));
+    unsigned int w[8] = {};
+    cudaError_t ce = cudaMemset(d_w, 0, 8 * sizeof(unsigned int));
+    const long long blocks = std::max<long long>(1, std::min<long long>((n + 255) / 256, 4096));
+    if (ce == cudaSuccess) {
+        nb_slot_kinds<T><<<(unsigned)blocks, 256>>>(n, (const int32_t*)h.nb, (const T*)h.coef, (const T*)h.cw,
+                                                    (const uint8_t*)h.m6, d_w);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpy(w, d_w, 8 * sizeof(unsigned int), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && !(w[0] & 1u) && !(w[1] & 2u)) {
+        const long long nblk = h.ldv / 512;
+        ce = cudaMalloc((void**)&h.nbr, (size_t)h.ldv * 4 * sizeof(int16_t));
+        if (ce == cudaSuccess) ce = cudaMalloc((void**)&h.nbase, (size_t)nblk * 4 * sizeof(int32_t));
+        if (ce == cudaSuccess) ce = cudaMemset(d_w + 6, 0, sizeof(unsigned int));
+        if (ce == cudaSuccess) {
+            nb_compact<T><<<(unsigned)nblk, 256>>>(n, (const int32_t*)h.nb, (const T*)h.coef, (const T*)h.cw,
+                                                   (const uint8_t*)h.m6, h.nbr, h.nbase, d_w + 6);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpy(w + 6, d_w + 6, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess || w[6] != 0u) {
+            if (h.nbr) cudaFree(h.nbr);
+            if (h.nbase) cudaFree(h.nbase);
+            h.nbr = nullptr;
+            h.nbase = nullptr;
+        }
+    }
+    cudaFree(d_w);
+    if (ce != cudaSuccess) { set_last_error("build_compact_nb", ce); return PHS_ERR_CUDA; }
+    return PHS_OK;
+}
+
 template <typename T>
 int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     int rc = validate_desc(d);
@@ -1479,6 +1636,10 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     h.n_tiles = (int)((h.n + tile - 1) / tile);
     h.m = (int)std::min<long long>(d->restart, h.n);
     const size_t n = (size_t)h.n;
+    // per-voxel arrays hold a whole number of the largest tile (zero tail), so
+    // a tile's slice of any of them can be copied whole
+    const size_t np = (n + kPadVoxels - 1) / kPadVoxels * kPadVoxels;
+    h.ldv = (long long)np;
     auto fail = [&](int code) { free_inst(h); return code; };
 #define PHS_ALLOC(ptr, bytes)                                            \
     do {                                                                 \
@@ -1487,25 +1648,31 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     } while (0)
     // tables: host arrays, or device arrays when device_tables (cudaMemcpyDefault)
     const bool dev = d->device_tables != 0;
-    PHS_ALLOC(h.nb, n * 6 * sizeof(int32_t));
-    if (cudaMemcpy(h.nb, d->nb6, n * 6 * sizeof(int32_t), cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
+    auto copy_in = [&](void* dst, const void* src, size_t bytes, size_t alloc_bytes) {
+        if (alloc_bytes > bytes && cudaMemset((char*)dst + bytes, 0, alloc_bytes - bytes) != cudaSuccess) return false;
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess;
+    };
+    PHS_ALLOC(h.nb, np * 6 * sizeof(int32_t));
+    if (!copy_in(h.nb, d->nb6, n * 6 * sizeof(int32_t), np * 6 * sizeof(int32_t))) return fail(PHS_ERR_CUDA);
     if (d->cw) {
-        if ((rc = upload_converted<T>(&h.cw, d->cw, (long long)n, dev)) != PHS_OK) return fail(rc);
-        PHS_ALLOC(h.m6, n);
-        if (cudaMemcpy(h.m6, d->mask6, n, cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
+        if ((rc = upload_converted<T>(&h.cw, d->cw, (long long)n, dev, (long long)np)) != PHS_OK) return fail(rc);
+        PHS_ALLOC(h.m6, np);
+        if (!copy_in(h.m6, d->mask6, n, np)) return fail(PHS_ERR_CUDA);
     } else {
-        if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6, dev)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.coef, d->coef6, (long long)n * 6, dev, (long long)np * 6)) != PHS_OK)
+            return fail(rc);
     }
     if (d->nb_edge) {
-        PHS_ALLOC(h.enb, n * 12 * sizeof(int32_t));
-        if (cudaMemcpy(h.enb, d->nb_edge, n * 12 * sizeof(int32_t), cudaMemcpyDefault) != cudaSuccess)
-            return fail(PHS_ERR_CUDA);
-        if ((rc = upload_converted<T>(&h.ecf, d->coef_edge, (long long)n * 6, dev)) != PHS_OK) return fail(rc);
+        PHS_ALLOC(h.enb, np * 12 * sizeof(int32_t));
+        if (!copy_in(h.enb, d->nb_edge, n * 12 * sizeof(int32_t), np * 12 * sizeof(int32_t))) return fail(PHS_ERR_CUDA);
+        if ((rc = upload_converted<T>(&h.ecf, d->coef_edge, (long long)n * 6, dev, (long long)np * 6)) != PHS_OK)
+            return fail(rc);
     }
-    PHS_ALLOC(h.vflags, n);
-    if (cudaMemcpy(h.vflags, d->vflags, n, cudaMemcpyDefault) != cudaSuccess) return fail(PHS_ERR_CUDA);
+    PHS_ALLOC(h.vflags, np);
+    if (!copy_in(h.vflags, d->vflags, n, np)) return fail(PHS_ERR_CUDA);
     if (d->vparams) {
-        if ((rc = upload_converted<T>(&h.vparams, d->vparams, (long long)n * 5, dev)) != PHS_OK) return fail(rc);
+        if ((rc = upload_converted<T>(&h.vparams, d->vparams, (long long)n * 5, dev, (long long)np * 5)) != PHS_OK)
+            return fail(rc);
     }
     if (dev) {
         // the checks validate_desc makes on host tables, on the copies
@@ -1525,6 +1692,7 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
         if (ce != cudaSuccess) { set_last_error("check_tables", ce); return fail(PHS_ERR_CUDA); }
         if (h_err) return fail(PHS_ERR_BAD_TABLE);
     }
+    if ((rc = build_compact_nb<T>(h)) != PHS_OK) return fail(rc);
     const size_t ns = (size_t)std::max<int64_t>(d->n_steps, 1);
     PHS_ALLOC(h.stim, ns);
     if (d->n_steps > 0) {
@@ -1532,17 +1700,17 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     } else {
         cudaMemset(h.stim, 0, ns);
     }
-    PHS_ALLOC(h.u, n * sizeof(T));
-    PHS_ALLOC(h.h0, n * sizeof(T));
-    PHS_ALLOC(h.h1, n * sizeof(T));
-    PHS_ALLOC(h.x, n * sizeof(T));
-    PHS_ALLOC(h.b, n * sizeof(T));
-    PHS_ALLOC(h.V, n * (size_t)(h.m + 1) * sizeof(T));
-    if (d->guess) PHS_ALLOC(h.dx, n * sizeof(T));
+    PHS_ALLOC(h.u, np * sizeof(T));
+    PHS_ALLOC(h.h0, np * sizeof(T));
+    PHS_ALLOC(h.h1, np * sizeof(T));
+    PHS_ALLOC(h.x, np * sizeof(T));
+    PHS_ALLOC(h.b, np * sizeof(T));
+    PHS_ALLOC(h.V, np * (size_t)(h.m + 1) * sizeof(T));
+    if (d->guess) PHS_ALLOC(h.dx, np * sizeof(T));
     const size_t S = (size_t)std::max(d->n_samples, 1);
     PHS_ALLOC(h.hist_u, S * n * sizeof(T));
     if (d->save_h) PHS_ALLOC(h.hist_h, S * n * sizeof(T));
-    PHS_ALLOC(h.lat, n * sizeof(int32_t));
+    PHS_ALLOC(h.lat, np * sizeof(int32_t));
     const size_t nparts = (size_t)h.n_tiles * (kWarpParts<T> ? kWarps : 1);
     PHS_ALLOC(h.part, nparts * (h.m + 2) * sizeof(double));
     h.n_groups = (h.n_tiles + kGroupTiles - 1) / kGroupTiles;
@@ -1554,16 +1722,16 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
     PHS_ALLOC(h.sync, sizeof(TeamSync));
     PHS_ALLOC(h.st, sizeof(InstState));
 #undef PHS_ALLOC
-    fill_dev<T>((T*)h.u, (long long)n, (T)d->u0, 0);
-    fill_dev<T>((T*)h.h0, (long long)n, (T)d->h0, 0);
-    fill_dev<T>((T*)h.h1, (long long)n, (T)d->h0, 0);
-    fill_dev<T>((T*)h.x, (long long)n, (T)0, 0);
-    fill_dev<T>((T*)h.b, (long long)n, (T)0, 0);
-    cudaMemset(h.V, 0, n * (size_t)(h.m + 1) * sizeof(T));
-    if (h.dx) cudaMemset(h.dx, 0, n * sizeof(T));
+    fill_dev<T>((T*)h.u, (long long)np, (T)d->u0, 0);
+    fill_dev<T>((T*)h.h0, (long long)np, (T)d->h0, 0);
+    fill_dev<T>((T*)h.h1, (long long)np, (T)d->h0, 0);
+    fill_dev<T>((T*)h.x, (long long)np, (T)0, 0);
+    fill_dev<T>((T*)h.b, (long long)np, (T)0, 0);
+    cudaMemset(h.V, 0, np * (size_t)(h.m + 1) * sizeof(T));
+    if (h.dx) cudaMemset(h.dx, 0, np * sizeof(T));
     cudaMemset(h.hist_u, 0, S * n * sizeof(T));
     if (h.hist_h) cudaMemset(h.hist_h, 0, S * n * sizeof(T));
-    cudaMemset(h.lat, 0xff, n * sizeof(int32_t));
+    cudaMemset(h.lat, 0xff, np * sizeof(int32_t));
     cudaMemset(h.part, 0, nparts * (h.m + 2) * sizeof(double));
     if (h.gpart) cudaMemset(h.gpart, 0, (size_t)h.n_groups * (h.m + 2) * sizeof(double));
     if (h.gcnt) cudaMemset(h.gcnt, 0, (size_t)h.n_groups * sizeof(unsigned int));
@@ -1598,9 +1766,13 @@ int add_instance(phs_engine* e, const phs_instance_desc* d, int* slot) {
 }
 
 template <typename T>
-InstDev<T> make_dev(const InstHost& h, bool group_sums, int vpt) {
+InstDev<T> make_dev(const InstHost& h, bool group_sums, int vpt, bool compact_nb) {
     InstDev<T> I{};
     I.nb = (const int32_t*)h.nb;
+    if (compact_nb && h.nbr) {
+        I.nbr = h.nbr;
+        I.nbase = h.nbase;
+    }
     I.coef = (const T*)h.coef;
     I.cw = (const T*)h.cw;
     I.m6 = (const uint8_t*)h.m6;
@@ -1615,6 +1787,7 @@ InstDev<T> make_dev(const InstHost& h, bool group_sums, int vpt) {
     I.x = (T*)h.x;
     I.b = (T*)h.b;
     I.V = (T*)h.V;
+    I.ldv = h.ldv;
     I.dx = (T*)h.dx;
     I.hist_u = (T*)h.hist_u;
     I.hist_h = (T*)h.hist_h;
@@ -1738,7 +1911,7 @@ int build_plan(phs_engine* e, int cps, bool edge) {
     std::vector<InstDev<T>> descs;
     descs.reserve(act.size());
     const int vpt = vpt_of((int)sizeof(T), variant_of<T>(e));
-    for (int i : act) descs.push_back(make_dev<T>(e->inst[i], e->group_sums, vpt));
+    for (int i : act) descs.push_back(make_dev<T>(e->inst[i], e->group_sums, vpt, e->compact_nb));
     size_t bytes = descs.size() * sizeof(InstDev<T>);
     if (bytes > e->d_desc_bytes) {
         if (e->d_desc) cudaFree(e->d_desc);
@@ -2043,6 +2216,13 @@ int phs_instance_profile(phs_engine* e, int slot, uint64_t* out16) {
     return PHS_OK;
 }
 
+int phs_instance_table_bytes(phs_engine* e, int slot, int32_t* bytes_per_voxel) {
+    if (!e || !bytes_per_voxel || slot < 0 || slot >= (int)e->inst.size() || !e->inst[slot].used)
+        return PHS_ERR_BAD_ARG;
+    *bytes_per_voxel = (e->compact_nb && e->inst[slot].nbr) ? 8 : 24;
+    return PHS_OK;
+}
+
 int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, int32_t* max_regs) {
     if (precision != PHS_PREC_F32 && precision != PHS_PREC_F64) return PHS_ERR_BAD_ARG;
     const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
@@ -2116,6 +2296,12 @@ int phs_engine_config(phs_engine* e, int key, int64_t value) {
         case PHS_CFG_GROUP_SUMS:
             if (e->group_sums != (value != 0)) {
                 e->group_sums = value != 0;
+                e->dirty = true;
+            }
+            return PHS_OK;
+        case PHS_CFG_COMPACT_NB:
+            if (e->compact_nb != (value != 0)) {
+                e->compact_nb = value != 0;
                 e->dirty = true;
             }
             return PHS_OK;

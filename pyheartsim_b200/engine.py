@@ -208,11 +208,16 @@ class BatchedEngine:
     def config(self, key, value):
         _lib.check(_lib.lib().phs_engine_config(self._h, int(key), int(value)), "phs_engine_config")
 
-    def configure(self, variant=None, ctas_per_sm=None, auto_balance=None, wave_instances=None):
+    def configure(self, variant=None, ctas_per_sm=None, auto_balance=None, wave_instances=None,
+                  compact_nb=None):
         """Select the step-kernel variant and the CTAs per SM used by advance(),
-        whether the 2nd and 3rd advance after an add/remove rebalance first, and
-        the most instances per launch wave (0: all in one wave)."""
+        whether the 2nd and 3rd advance after an add/remove rebalance first,
+        the most instances per launch wave (0: all in one wave) and whether
+        instances read their compact neighbour table (same results)."""
         L = _lib.lib()
+        if compact_nb is not None:
+            _lib.check(L.phs_engine_config(self._h, _lib.CFG_COMPACT_NB, int(bool(compact_nb))),
+                       "phs_engine_config")
         if wave_instances is not None:
             _lib.check(L.phs_engine_config(self._h, _lib.CFG_WAVE_INSTANCES, int(wave_instances)),
                        "phs_engine_config")
@@ -239,6 +244,13 @@ class BatchedEngine:
         for i, name in enumerate(_lib.PROFILE_SLOTS):
             d[name] = int(out[i]) if name in ("steps", "arnoldi_iters", "team_ctas") else out[i] / 1e6
         return d
+
+    def table_bytes(self, slot):
+        """Bytes per voxel of the neighbour table the instance's compact-table
+        variants read (8 compact, 24 int32)."""
+        b = ctypes.c_int32()
+        _lib.check(_lib.lib().phs_instance_table_bytes(self._h, slot, ctypes.byref(b)), "phs_instance_table_bytes")
+        return int(b.value)
 
     def launches(self):
         return int(_lib.lib().phs_engine_launch_count(self._h))
