@@ -34,6 +34,7 @@ METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99
 # dram__bytes_write.sum of the two timed full-size launches of this batch, 2.71
 # Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md);
 # multiplied by the voxels and steps of one launch below.
+DEFAULT_F32_VARIANT = 2        # the engine's FP32 default when the autotuner is off
 STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 267.0
 STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.71
 BALANCE_LAUNCHES = 10   # launches per team-balancing round in the pre-steps
@@ -267,8 +268,12 @@ def run_b200(args):
     solves = np.array([b["solves"] - a["solves"] for a, b in zip(info0, info1)], dtype=np.float64)
     iso = [x.cw is not None for x in insts]
     gs = [bool(x.guess) for x in insts]
-    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, io, g)
-                          for n, ks, kq, sv, io, g in zip(ns, k_sum, k_sq, solves, iso, gs)))
+    # neighbour-table bytes per row: the compact table where the variant reads it
+    from pyheartsim_b200.engine import step_variant_layout
+    reads_compact = step_variant_layout(_lib.PREC_F32)[step_variant_of(tune)][1]
+    nbb = [roofline.COMPACT_NB if (reads_compact and eng.table_bytes(s) == 8) else 24 for s in slots]
+    alg_bytes = float(sum(roofline.algorithmic_bytes(4, int(n), K, ks, kq, sv, io, g, nb=nb)
+                          for n, ks, kq, sv, io, g, nb in zip(ns, k_sum, k_sq, solves, iso, gs, nbb)))
     local_vs = float(ns.sum()) * K
     total_vs = local_vs * world
     value = total_vs / (ms_max / 1e3)
@@ -327,15 +332,22 @@ def run_b200(args):
     return 0
 
 
+def step_variant_of(tune):
+    return tune["best"][0] if tune is not None else DEFAULT_F32_VARIANT
+
+
 def step_kernel_name(tune):
     """Template arguments (value type, voxels per thread, minimum CTAs per SM,
-    edge terms) of the step-kernel variant the timed launches used."""
-    from pyheartsim_b200.engine import step_variants
+    edge terms, staging ring bytes, compact table) of the step-kernel variant
+    the timed launches used."""
+    from pyheartsim_b200.engine import step_variants, step_variant_layout
     from pyheartsim_b200 import _lib
     var = {v: (minb, vpt) for v, minb, _, vpt in step_variants(_lib.PREC_F32, with_vpt=True)}
-    v = tune["best"][0] if tune is not None else 2
+    lay = step_variant_layout(_lib.PREC_F32)
+    v = step_variant_of(tune)
     minb, vpt = var[v]
-    return f"step_kernel<float,{vpt},{minb},false>"
+    ring, comp = lay[v]
+    return f"step_kernel<float,{vpt},{minb},false,{ring},{str(comp and ring == 0).lower()}>"
 
 
 def phase_profile(eng, slots, S, stream):

@@ -181,6 +181,13 @@ int phs_step_variants(int precision, int32_t* count, int32_t* min_ctas_per_sm, i
 /* Voxels per thread of each step-kernel variant of a precision (a tile is 256 x
  * that many consecutive voxels); vpt must hold `count` >= the variant count.   */
 int phs_step_variant_vpt(int precision, int32_t count, int32_t* vpt);
+/* Per variant: bytes of the shared-memory staging ring (0: the variant reads
+ * global memory directly; > 0: a producer warp copies each tile's slices into
+ * the ring with 1-D bulk copies) and whether it reads the compact neighbour
+ * table (PHS_CFG_COMPACT_NB; an unstaged variant that needs it for every
+ * instance runs its int32-table twin when one lacks it).  Arrays of at least
+ * count entries, may be NULL.                                                  */
+int phs_step_variant_layout(int precision, int32_t count, int32_t* ring_bytes, int32_t* compact_table);
 /* Re-split the CTAs over the instances in proportion to their cost since the
  * last rebalance: the measured team time per step x team CTAs when the phase
  * timers (PHS_CFG_PROFILE) are on, else voxels x (1.6 + Arnoldi iterations per

@@ -156,6 +156,7 @@ SIGNATURES = {
     "phs_engine_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64]),
     "phs_step_variants": (ctypes.c_int, [ctypes.c_int, c_int32_p, c_int32_p, c_int32_p]),
     "phs_step_variant_vpt": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, c_int32_p]),
+    "phs_step_variant_layout": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, c_int32_p, c_int32_p]),
     "phs_instance_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "phs_engine_rebalance": (ctypes.c_int, [ctypes.c_void_p]),
     "phs_instance_table_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int32_p]),

@@ -228,6 +228,179 @@ __device__ __forceinline__ unsigned long long global_ns() {
 constexpr unsigned long long kWaitNs = 4000000000ull;
 constexpr unsigned int kWaitPolls = 1u << 26;
 
+// Bulk L2 prefetch of [p, p + bytes) (p 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
+    const unsigned long long g = (unsigned long long)__cvta_generic_to_global(p);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
+}
+
+// ------------------------------------------------------------------ staging ring
+// Staged step kernels (RING > 0) add one producer warp to the 256 consumer
+// threads.  For every tile loop of a phase the consumers publish a job (the
+// arrays the phase streams and their bytes per voxel); the producer copies
+// each of the CTA's tiles' contiguous slices of every array into a stage of a
+// shared-memory ring with 1-D cp.async.bulk, signalled on the stage's "full"
+// mbarrier, and refills a stage once all consumer warps have arrived on its
+// "empty" mbarrier.  Consumers read the tile from shared memory; the stencil's
+// neighbour gathers and the scattered accesses stay on global memory.
+constexpr int kStageMaxArr = 12;    // arrays per stage
+constexpr int kMaxStages = 6;       // ring depth limit
+constexpr int kRingHeader = 1024;   // barriers and jobs ahead of the ring in dynamic shared memory
+
+struct StageJob {
+    const char* src[kStageMaxArr];  // array base (voxel 0)
+    int bytes[kStageMaxArr];        // bytes of one tile's slice
+    int off[kStageMaxArr];          // offset of the slice in a stage
+    int n_arr;
+    int stage_bytes;
+    int n_stages;
+    int tile0, step, n_tiles;       // the CTA's tiles: tile0, tile0 + step, ... < n_tiles
+    int quit;
+};
+struct RingHeader {
+    unsigned long long full[kMaxStages];
+    unsigned long long empty[kMaxStages];
+    StageJob job[2];
+    int stop;                       // a bounded stage wait gave up: later waits return at once
+};
+static_assert(sizeof(RingHeader) <= kRingHeader, "ring header");
+
+// Consumer-only CTA barrier: __syncthreads without a producer warp, else named
+// barrier 1 over the 256 consumer threads.
+template <bool ST>
+__device__ __forceinline__ void csync() {
+    if constexpr (ST) asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+    else __syncthreads();
+}
+// Job hand-over on named barrier 2: consumers arrive, the producer waits.
+__device__ __forceinline__ void job_arrive() { asm volatile("bar.arrive 2, %0;" ::"n"(kThreads + 32) : "memory"); }
+__device__ __forceinline__ void job_wait() { asm volatile("bar.sync 2, %0;" ::"n"(kThreads + 32) : "memory"); }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint32_t a, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// Bounded wait for the phase of parity `parity` of the mbarrier at a.  Gives up
+// after 4 s or 2^26 polls (sets *stop and the abort word), and at once once
+// *stop is set when `heed_stop`; returns whether the phase completed.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* stop, unsigned int* abort_word,
+                                          bool heed_stop = true) {
+    if (mbar_try(a, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned int polls = 0;; ++polls) {
+        if (mbar_try(a, parity)) return true;
+        if (heed_stop && *stop) return false;
+        if (polls > kWaitPolls || global_ns() - t0 > kWaitNs) {
+            *stop = 1;
+            atomicOr(abort_word, 1u);
+            return false;
+        }
+    }
+}
+// 1-D bulk copy global -> shared (both 16-byte aligned, bytes a multiple of 16),
+// completion counted on the mbarrier at mbar.  No multicast.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+// Orders this thread's generic-proxy global accesses before later async-proxy
+// (bulk copy) ones.
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+
+// Consumer side of the staging ring.  A phase lists its arrays with add()
+// (every consumer thread makes the same calls, so all agree on the offsets;
+// thread 0 writes the job), then publish() hands the job to the producer and
+// returns the ring depth, 0 when the phase runs unstaged; acquire() waits for
+// the next tile's stage and release() marks the calling warp done with it.
+template <int RING, int TILE, typename T>
+struct Stager {
+    RingHeader* rh;
+    unsigned char* ring;
+    int job_buf;
+    int lay_off, lay_n;
+    int nst, sg;          // ring depth of the phase, stage of the current tile
+    unsigned int cpar;    // parity to wait for on each full barrier
+
+    __device__ __forceinline__ void begin() {
+        lay_off = 0;
+        lay_n = 0;
+    }
+    __device__ __forceinline__ int add(const void* base, int elem) {
+        const int o = lay_off;
+        if (threadIdx.x == 0 && lay_n < kStageMaxArr) {
+            StageJob& J = rh->job[job_buf];
+            J.src[lay_n] = static_cast<const char*>(base);
+            J.bytes[lay_n] = TILE * elem;
+            J.off[lay_n] = o;
+        }
+        lay_off += TILE * elem;
+        ++lay_n;
+        return o;
+    }
+    // basis vectors a phase may stage after its fixed arrays: as many as keep
+    // the ring at least two stages deep
+    __device__ __forceinline__ int vec_cap() const {
+        const int c = (RING / 2 - lay_off) / (TILE * (int)sizeof(T));
+        return max(0, min(c, kStageMaxArr - lay_n));
+    }
+    __device__ __forceinline__ int publish(int rank, int P, int n_tiles) {
+        nst = (lay_off > 0 && lay_n <= kStageMaxArr) ? RING / lay_off : 0;
+        if (nst > kMaxStages) nst = kMaxStages;
+        if (rank >= n_tiles) nst = 0;
+        if (nst == 0) return 0;
+        if (threadIdx.x == 0) {
+            StageJob& J = rh->job[job_buf];
+            J.n_arr = lay_n;
+            J.stage_bytes = lay_off;
+            J.n_stages = nst;
+            J.tile0 = rank;
+            J.step = P;
+            J.n_tiles = n_tiles;
+            J.quit = 0;
+        }
+        fence_proxy_async_global();   // this thread's global writes before the bulk reads
+        csync<true>();
+        job_arrive();
+        job_buf ^= 1;
+        sg = -1;
+        return nst;
+    }
+    __device__ __forceinline__ const unsigned char* acquire(unsigned int* abort_word) {
+        if (++sg == nst) sg = 0;
+        mbar_wait(smem_u32(&rh->full[sg]), (cpar >> sg) & 1u, &rh->stop, abort_word);
+        cpar ^= 1u << sg;
+        return ring + sg * lay_off;
+    }
+    __device__ __forceinline__ void release() {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(smem_u32(&rh->empty[sg]));
+    }
+    // hands the producer warp its last job
+    __device__ __forceinline__ void quit() {
+        if (threadIdx.x == 0) rh->job[job_buf].quit = 1;
+        csync<true>();
+        job_arrive();
+    }
+};
+
 struct SharedCtl {
     int last;
     unsigned int gen;
@@ -241,10 +414,10 @@ struct SharedCtl {
 // Bounded team barrier.  The last CTA to arrive runs `leader` (whole CTA)
 // before releasing the others.  Returns false when the wait gave up or another
 // team aborted; the kernel then leaves all loops.
-template <typename Leader>
+template <bool ST, typename Leader>
 __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abort_word, SharedCtl& ctl,
                                           Leader&& leader) {
-    __syncthreads();
+    csync<ST>();
     if (threadIdx.x == 0) {
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(ts->count);
@@ -256,10 +429,10 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
         ctl.abort = 0;
         if (ctl.last) __threadfence();
     }
-    __syncthreads();
+    csync<ST>();
     if (ctl.last) {
         leader();
-        __syncthreads();
+        csync<ST>();
         if (threadIdx.x == 0) {
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(ts->count);
@@ -283,7 +456,7 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
         }
         __threadfence();
     }
-    __syncthreads();
+    csync<ST>();
     return ctl.abort == 0;
 }
 
@@ -368,11 +541,6 @@ __device__ __forceinline__ T edge_row(const T* vec, const int32_t* enb, const T*
     return acc;
 }
 
-// Bulk L2 prefetch of [p, p + bytes) (p 16-byte aligned, bytes a multiple of 16).
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned int bytes) {
-    const unsigned long long g = (unsigned long long)__cvta_generic_to_global(p);
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g), "r"(bytes) : "memory");
-}
 
 // Basis vectors whose loads are issued together: FP32 tiles hold four voxels
 // per thread (four loads per vector already), FP64 tiles one, and the FP64
@@ -391,10 +559,14 @@ constexpr int kMaxGroupWalk = 32;   // tiles a CTA counts in per pass
 // ------------------------------------------------------------------ the kernel
 // EDGE: the launch carries anisotropic instances (edge cross terms); the
 // isotropic launches compile without that code.
-template <typename T, int VPT, int MINB, bool EDGE>
-__global__ void __launch_bounds__(kThreads, MINB)
+template <typename T, int VPT, int MINB, bool EDGE, int RING, bool NBC>
+__global__ void __launch_bounds__(kThreads + (RING > 0 ? 32 : 0), MINB)
 step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_map,
             long long n_steps_launch, unsigned int* abort_word) {
+    constexpr bool ST = RING > 0;   // staged: producer warp + shared-memory ring (FP32 only)
+    static_assert(!ST || sizeof(T) == 4, "staged kernels are FP32");
+    // NBC: every instance of the launch has a compact neighbour table (decode_nb)
+    static_assert(!(ST && NBC), "staged kernels choose the table per instance");
     constexpr int TILE = kThreads * VPT;
     constexpr int kChunk = kChunkOf<T>;
     const int4 cm = cta_map[blockIdx.x];
@@ -406,6 +578,10 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     __shared__ double shc[kMaxRestart + 1];
     __shared__ long long sh_step0;
     __shared__ int sh_id_save, sh_pending, sh_hbuf, sh_status;
+    // staged kernels: ring header (mbarriers, jobs) and the ring itself
+    extern __shared__ __align__(128) unsigned char dyn_smem[];
+    RingHeader* const rh = reinterpret_cast<RingHeader*>(dyn_smem);
+    unsigned char* const ring = dyn_smem + kRingHeader;
 
     if (threadIdx.x == 0) {
         I = insts[cm.x];
@@ -414,8 +590,66 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         sh_pending = __ldcg(&I.st->pending);
         sh_hbuf = __ldcg(&I.st->hbuf);
         sh_status = __ldcg(&I.st->status);
+        if constexpr (ST) {
+            for (int q = 0; q < kMaxStages; ++q) {
+                mbar_init(smem_u32(&rh->full[q]), 1u);
+                mbar_init(smem_u32(&rh->empty[q]), (unsigned)kWarps);
+            }
+            rh->stop = 0;
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
     }
     __syncthreads();
+
+    if constexpr (ST) {
+        // ---- producer warp: copies the slices of each published job's tiles
+        if (threadIdx.x >= kThreads) {
+            const int pl = threadIdx.x - kThreads;
+            const uint32_t ring_u32 = smem_u32(ring);
+            volatile int* stop = &rh->stop;
+            unsigned int epar = 0xffffffffu;   // parity to wait for on each empty barrier (fresh: passes)
+            unsigned int fpar = 0u;            // fills of each stage, mod 2
+            unsigned int used = 0u;
+            bool dead = false;                 // an empty-barrier wait gave up: issue nothing more
+            int jb = 0;
+            for (;;) {
+                job_wait();
+                const StageJob* J = &rh->job[jb];
+                jb ^= 1;
+                if (J->quit) break;
+                fence_proxy_async_global();
+                const int na = J->n_arr, sbytes = J->stage_bytes, nst = J->n_stages;
+                const int tstep = J->step, nt = J->n_tiles;
+                const char* src = pl < na ? J->src[pl] : nullptr;
+                const int bytes = pl < na ? J->bytes[pl] : 0;
+                const int off = pl < na ? J->off[pl] : 0;
+                int sg = 0;
+                for (int tile = J->tile0; tile < nt && !dead; tile += tstep) {
+                    const uint32_t fb = smem_u32(&rh->full[sg]);
+                    bool ok = true;
+                    if (pl == 0) ok = mbar_wait(smem_u32(&rh->empty[sg]), (epar >> sg) & 1u, stop, abort_word);
+                    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                    if (!ok) {
+                        dead = true;
+                        break;
+                    }
+                    epar ^= 1u << sg;
+                    if (pl == 0) mbar_expect_tx(fb, (uint32_t)sbytes);
+                    __syncwarp();
+                    if (pl < na) bulk_g2s(ring_u32 + (uint32_t)(sg * sbytes + off), src + (size_t)tile * bytes, (uint32_t)bytes, fb);
+                    fpar ^= 1u << sg;
+                    used |= 1u << sg;
+                    if (++sg == nst) sg = 0;
+                }
+            }
+            // every copy this CTA issued has landed before it exits
+            if (pl == 0)
+                for (int q = 0; q < kMaxStages; ++q)
+                    if ((used >> q) & 1u) mbar_wait(smem_u32(&rh->full[q]), ((fpar >> q) & 1u) ^ 1u, stop, abort_word, false);
+            __syncwarp();
+            return;
+        }
+    }
 
     const long long N = I.n;
     const int ps = I.ps;
@@ -464,7 +698,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
     auto tile_done = [&](int tile, int nslot) {
         if constexpr (!kWarpParts<T>) {
-            __syncthreads();
+            csync<ST>();
             for (int t = threadIdx.x; t < nslot; t += kThreads) {
                 double a = 0.0;
 #pragma unroll
@@ -485,7 +719,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         if constexpr (!kWarpParts<T>) {
             if (I.gpart == nullptr) return;
             for (int base = rank; base < I.n_tiles; base += kMaxGroupWalk * P) {
-                __syncthreads();
+                csync<ST>();
                 if (threadIdx.x == 0) {
                     __threadfence();
                     int nl = 0;
@@ -499,7 +733,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     sh_nlast = nl;
                     __threadfence();
                 }
-                __syncthreads();
+                csync<ST>();
                 for (int q = 0; q < sh_nlast; ++q) {
                     const int g = sh_glast[q];
                     const int t0 = g * kGroupTiles;
@@ -515,6 +749,40 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
     };
     auto voxel = [&](int tile, int v) -> long long { return (long long)tile * TILE + v * kThreads + threadIdx.x; };
+
+    // ---- consumer side of the staging ring (ST)
+    Stager<RING, TILE, T> stg{rh, ring, 0, 0, 0, 0, 0, 0u};
+    // row coefficients of local voxel li from a stage (cw + m6, or coef)
+    auto stage_coef = [&](const unsigned char* sb, int o_c, int o_m, int li, T (&c)[6]) {
+        if (o_m >= 0) {
+            const T w = reinterpret_cast<const T*>(sb + o_c)[li];
+            const unsigned mk = sb[o_m + li];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) c[k] = ((mk >> k) & 1u) ? w : T(0);
+        } else {
+            const T* cf = reinterpret_cast<const T*>(sb + o_c) + 6 * li;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) c[k] = cf[k];
+        }
+    };
+    // neighbour indices of voxel n (local li) from a stage's compact table, or
+    // the int32 table in global memory when the instance has none
+    auto stage_nb = [&](const unsigned char* sb, int o_nb, int li, long long n, int32_t (&q)[6]) {
+        if (o_nb >= 0)
+            decode_nb(reinterpret_cast<const short4*>(sb + o_nb)[li], __ldg(reinterpret_cast<const int4*>(I.nbase) + (n >> 9)),
+                      n, q);
+        else
+            load_nb(I.nb, n, q);
+    };
+    // neighbour indices of row n (unstaged loops)
+    auto row_nb = [&](long long n, int32_t (&q)[6]) {
+        if constexpr (NBC) {
+            decode_nb(__ldg(reinterpret_cast<const short4*>(I.nbr) + n), __ldg(reinterpret_cast<const int4*>(I.nbase) + (n >> 9)),
+                      n, q);
+        } else {
+            load_nb(I.nb, n, q);
+        }
+    };
 
     // Prefetch into L2 the slice of an array (elem bytes per voxel) that `tile`
     // will read, so that the loads of the CTA's next tile find it there.  Start
@@ -533,7 +801,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     // the row tables of the operator (neighbours, coefficients, flags, edges)
     auto pf_rows = [&](int t, int tile) {
         switch (t) {
-            case 0: pf_slice(I.nb, 24, tile); break;
+            case 0: if (NBC) pf_slice(I.nbr, 8, tile); else pf_slice(I.nb, 24, tile); break;
             case 1: pf_slice(I.cw ? (const void*)I.cw : (const void*)I.coef, I.cw ? (int)sizeof(T) : 6 * (int)sizeof(T), tile); break;
             case 2: pf_slice(I.m6, 1, tile); break;
             case 3: pf_slice(I.vflags, 1, tile); break;
@@ -584,14 +852,14 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 if (lane == 0 && s0 + u < ns) bsum_w[s0 + u][warp] = v;
             }
         }
-        __syncthreads();
+        csync<ST>();
         for (int i = threadIdx.x; i < ns; i += kThreads) {
             double t = 0.0;
 #pragma unroll
             for (int w = 0; w < kWarps; ++w) t += bsum_w[i][w];
             bsum_out[i] = t;
         }
-        __syncthreads();
+        csync<ST>();
     };
 
     // statistics of a solve that iterated, recorded by the leader that ends it
@@ -666,7 +934,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             gv_g[i] = __ldcg(sc->g + i);
             gv_s[i] = __ldcg(sc->s + i);
         }
-        __syncthreads();
+        csync<ST>();
         if (threadIdx.x == 0) {
             const double hn = sqrt(bsum_out[0]);
             gv_col[j + 1] = hn;
@@ -713,7 +981,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             sc->action = act;
             gv_act = act;
         }
-        __syncthreads();
+        csync<ST>();
         for (int i = threadIdx.x; i <= j + 1; i += kThreads) Rc[i] = gv_col[i];
         const int act = gv_act;
         if (act != ACT_UPDATE_FINAL && act != ACT_UPDATE_CHECK) return;
@@ -722,7 +990,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         for (int l = warp; l < k; l += kWarps)
             for (int i = lane; i <= l; i += 32)
                 gv_R[l * (l + 1) / 2 + i] = (l == j) ? gv_col[i] : __ldcg(sc->R + l * (kMaxRestart + 1) + i);
-        __syncthreads();
+        csync<ST>();
         if (warp == 0) {
             for (int i = k - 1; i >= 0; --i) {
                 double acc = 0.0;
@@ -772,14 +1040,14 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             ctl.action = __ldcg(&sc->action);
             ctl.k = __ldcg(&sc->k);
         }
-        __syncthreads();
+        csync<ST>();
         return ctl.action;
     };
 
     auto load_shc = [&](int cnt) {
-        __syncthreads();
+        csync<ST>();
         for (int i = threadIdx.x; i < cnt; i += kThreads) shc[i] = __ldcg(sc->coef + i);
-        __syncthreads();
+        csync<ST>();
     };
 
     // ---- sample / activation bookkeeping of the state in u (after step s-1)
@@ -897,9 +1165,64 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         pending = -1;
         mark(PF_RHS1);
-        if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
         mark(PF_RHS_WAIT);
-        for (int tile = rank; tile < I.n_tiles; tile += P) {
+        int nst = 0;
+        if constexpr (ST) {
+            stg.begin();
+            const int o_us = stg.add(Us, sizeof(T));
+            const int o_nb = I.nbr ? stg.add(I.nbr, 8) : -1;
+            const int o_cw = I.cw ? stg.add(I.cw, sizeof(T)) : stg.add(I.coef, 6 * sizeof(T));
+            const int o_m6 = I.cw ? stg.add(I.m6, 1) : -1;
+            const int o_dx = I.dx ? stg.add(I.dx, sizeof(T)) : -1;
+            const int o_fl = tb ? stg.add(I.vflags, 1) : -1;
+            nst = stg.publish(rank, P, I.n_tiles);
+            for (int tile = rank; nst > 0 && tile < I.n_tiles; tile += P) {
+                const unsigned char* sb = stg.acquire(abort_word);
+                double ab = 0.0, ar = 0.0;
+#pragma unroll
+                for (int v = 0; v < VPT; ++v) {
+                    const int li = v * kThreads + threadIdx.x;
+                    const long long n = (long long)tile * TILE + li;
+                    if (n < N) {
+                        const T us = reinterpret_cast<const T*>(sb + o_us)[li];
+                        const bool rz = tb && (sb[o_fl + li] & PHS_VFLAG_TBLOCK);
+                        int32_t q[6];
+                        T c[6];
+                        stage_nb(sb, o_nb, li, n, q);
+                        stage_coef(sb, o_cw, o_m6, li, c);
+                        T lap = T(0), dp = T(0), lapd = T(0);
+                        if (!rz) {
+                            lap = lap_row(Us, us, q, c);
+                            if (EDGE && I.ecf) lap += edge_row(Us, I.enb, I.ecf, n);
+                        }
+                        if (o_dx >= 0) {
+                            dp = reinterpret_cast<const T*>(sb + o_dx)[li];
+                            if (!rz) {
+                                lapd = lap_row(I.dx, dp, q, c);
+                                if (EDGE && I.ecf) lapd += edge_row(I.dx, I.enb, I.ecf, n);
+                            }
+                        }
+                        const T x0 = us + dp;
+                        const T bn = us + I.half_dt * lap;
+                        const T ax = x0 - I.half_dt * (lap + lapd);
+                        const T rn = bn - ax;
+                        I.x[n] = x0;
+                        I.b[n] = bn;
+                        Vb[n] = rn;
+                        ab += (double)bn * (double)bn;
+                        ar += (double)rn * (double)rn;
+                    }
+                }
+                stg.release();
+                ab = warp_sum(ab);
+                ar = warp_sum(ar);
+                put(tile, 0, ab);
+                put(tile, 1, ar);
+                tile_done(tile, 2);
+            }
+        }
+        for (int tile = rank; nst == 0 && tile < I.n_tiles; tile += P) {
             if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
             else if (threadIdx.x == kRowArrays) pf_slice(Us, sizeof(T), tile + P);
             else if (threadIdx.x == kRowArrays + 1) pf_slice(I.dx, sizeof(T), tile + P);
@@ -912,7 +1235,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
                     int32_t q[6];
                     T c[6];
-                    load_nb(I.nb, n, q);
+                    row_nb(n, q);
                     row_coef(I.coef, I.cw, I.m6, n, c);
                     T lap = T(0), dp = T(0), lapd = T(0);
                     if (!rz) {
@@ -947,7 +1270,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         groups_done(2);
         mark(PF_RHS);
-        if (!team_sync(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
         int act = read_action();
         mark(PF_RHS_WAIT);
         // end of this step: its history slot, and whether the pass that writes
@@ -966,11 +1289,77 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 for (;;) {
                     // ============ phase A: w = A (s_j V_j) -> V_{j+1}; dots <V_i, w>
                     if (threadIdx.x == 0) ctl.sj = __ldcg(&sc->s[j]);
-                    __syncthreads();
+                    csync<ST>();
                     const T sj = (T)ctl.sj;
                     const T* Vj = Vb + (size_t)j * ldV;
                     T* Vn = Vb + (size_t)(j + 1) * ldV;
-                    for (int tile = rank; tile < I.n_tiles; tile += P) {
+                    int nsa = 0;
+                    if constexpr (ST) {
+                        stg.begin();
+                        const int o_vj = stg.add(Vj, sizeof(T));
+                        const int o_nb = I.nbr ? stg.add(I.nbr, 8) : -1;
+                        const int o_cw = I.cw ? stg.add(I.cw, sizeof(T)) : stg.add(I.coef, 6 * sizeof(T));
+                        const int o_m6 = I.cw ? stg.add(I.m6, 1) : -1;
+                        const int o_fl = tb ? stg.add(I.vflags, 1) : -1;
+                        const int nvs = min(j, stg.vec_cap());      // V_0 .. V_{nvs-1} staged too
+                        const int o_v = stg.lay_off;
+                        for (int i = 0; i < nvs; ++i) stg.add(Vb + (size_t)i * ldV, sizeof(T));
+                        nsa = stg.publish(rank, P, I.n_tiles);
+                        for (int tile = rank; nsa > 0 && tile < I.n_tiles; tile += P) {
+                            const unsigned char* sb = stg.acquire(abort_word);
+                            const T* vjs = reinterpret_cast<const T*>(sb + o_vj);
+                            T wr[VPT];
+#pragma unroll
+                            for (int v = 0; v < VPT; ++v) {
+                                const int li = v * kThreads + threadIdx.x;
+                                const long long n = (long long)tile * TILE + li;
+                                wr[v] = T(0);
+                                if (n < N) {
+                                    const T vj = vjs[li];
+                                    const bool rz = tb && (sb[o_fl + li] & PHS_VFLAG_TBLOCK);
+                                    int32_t q[6];
+                                    T c[6];
+                                    stage_nb(sb, o_nb, li, n, q);
+                                    stage_coef(sb, o_cw, o_m6, li, c);
+                                    T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
+                                    if (EDGE && I.ecf && !rz) lap += edge_row(Vj, I.enb, I.ecf, n);
+                                    const T w = sj * (vj - I.half_dt * lap);
+                                    Vn[n] = w;
+                                    wr[v] = w;
+                                }
+                            }
+                            for (int i0 = 0; i0 <= j; i0 += kChunk) {
+                                T vv[kChunk][VPT];
+#pragma unroll
+                                for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                                    for (int v = 0; v < VPT; ++v) {
+                                        const int li = v * kThreads + threadIdx.x;
+                                        const long long n = (long long)tile * TILE + li;
+                                        const int i = i0 + ii;
+                                        T val = T(0);
+                                        if (i <= j && n < N)
+                                            val = (i == j) ? vjs[li]
+                                                  : (i < nvs) ? reinterpret_cast<const T*>(sb + o_v + i * TILE * (int)sizeof(T))[li]
+                                                              : Vb[(size_t)i * ldV + n];
+                                        vv[ii][v] = val;
+                                    }
+#pragma unroll
+                                for (int ii = 0; ii < kChunk; ++ii) {
+                                    double d = 0.0;
+#pragma unroll
+                                    for (int v = 0; v < VPT; ++v) d += (double)vv[ii][v] * (double)wr[v];
+                                    if (i0 + ii <= j) {          // uniform over the warp
+                                        d = warp_sum(d);
+                                        put(tile, i0 + ii, d);
+                                    }
+                                }
+                            }
+                            stg.release();
+                            tile_done(tile, j + 1);
+                        }
+                    }
+                    for (int tile = rank; nsa == 0 && tile < I.n_tiles; tile += P) {
                         if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
                         else if (threadIdx.x <= kRowArrays + j)
                             pf_slice(Vb + (size_t)(threadIdx.x - kRowArrays) * ldV, sizeof(T), tile + P);
@@ -984,7 +1373,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                                 const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
                                 int32_t q[6];
                                 T c[6];
-                                load_nb(I.nb, n, q);
+                                row_nb(n, q);
                                 row_coef(I.coef, I.cw, I.m6, n, c);
                                 T lap = rz ? T(0) : lap_row(Vj, vj, q, c);
                                 if (EDGE && I.ecf && !rz) lap += edge_row(Vj, I.enb, I.ecf, n);
@@ -1017,11 +1406,68 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(j + 1);
                     mark(PF_A);
-                    if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_dots(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() { leader_dots(j); })) { aborted = true; break; }
                     load_shc(j + 1);
                     mark(PF_A_WAIT);
                     // ============ phase C: u = w - sum_i c_i V_i  (in place), ||u||^2
-                    for (int tile = rank; tile < I.n_tiles; tile += P) {
+                    int nsc = 0;
+                    if constexpr (ST) {
+                        stg.begin();
+                        const int o_w = stg.add(Vn, sizeof(T));
+                        const int nvs = min(j + 1, stg.vec_cap());
+                        const int o_v = stg.lay_off;
+                        for (int i = 0; i < nvs; ++i) stg.add(Vb + (size_t)i * ldV, sizeof(T));
+                        nsc = stg.publish(rank, P, I.n_tiles);
+                        for (int tile = rank; nsc > 0 && tile < I.n_tiles; tile += P) {
+                            const unsigned char* sb = stg.acquire(abort_word);
+                            double acc[VPT];
+#pragma unroll
+                            for (int v = 0; v < VPT; ++v) {
+                                const int li = v * kThreads + threadIdx.x;
+                                const long long n = (long long)tile * TILE + li;
+                                acc[v] = (n < N) ? (double)reinterpret_cast<const T*>(sb + o_w)[li] : 0.0;
+                            }
+                            for (int i0 = 0; i0 <= j; i0 += kChunk) {
+                                T vv[kChunk][VPT];
+#pragma unroll
+                                for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                                    for (int v = 0; v < VPT; ++v) {
+                                        const int li = v * kThreads + threadIdx.x;
+                                        const long long n = (long long)tile * TILE + li;
+                                        const int i = i0 + ii;
+                                        T val = T(0);
+                                        if (i <= j && n < N)
+                                            val = (i < nvs) ? reinterpret_cast<const T*>(sb + o_v + i * TILE * (int)sizeof(T))[li]
+                                                            : Vb[(size_t)i * ldV + n];
+                                        vv[ii][v] = val;
+                                    }
+#pragma unroll
+                                for (int ii = 0; ii < kChunk; ++ii) {
+                                    if (i0 + ii <= j) {
+                                        const double cf = shc[i0 + ii];
+#pragma unroll
+                                        for (int v = 0; v < VPT; ++v) acc[v] -= cf * (double)vv[ii][v];
+                                    }
+                                }
+                            }
+                            stg.release();
+                            double a2 = 0.0;
+#pragma unroll
+                            for (int v = 0; v < VPT; ++v) {
+                                const long long n = voxel(tile, v);
+                                if (n < N) {
+                                    const T ut = (T)acc[v];
+                                    Vn[n] = ut;
+                                    a2 += (double)ut * (double)ut;
+                                }
+                            }
+                            a2 = warp_sum(a2);
+                            put(tile, 0, a2);
+                            tile_done(tile, 1);
+                        }
+                    }
+                    for (int tile = rank; nsc == 0 && tile < I.n_tiles; tile += P) {
                         if (threadIdx.x <= j + 1) pf_slice(Vb + (size_t)threadIdx.x * ldV, sizeof(T), tile + P);
                         double acc[VPT];
 #pragma unroll
@@ -1064,7 +1510,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(1);
                     mark(PF_C);
-                    if (!team_sync(I.sync, P, abort_word, ctl, [&]() { leader_norm(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() { leader_norm(j); })) { aborted = true; break; }
                     act = read_action();
                     mark(PF_C_WAIT);
                     if (prof_on && threadIdx.x == 0) pf[PF_SOLVE_ITERS] += 1;
@@ -1078,7 +1524,86 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 load_shc(k);
                 const bool final = (act == ACT_UPDATE_FINAL);
                 const bool react = final && fuse_next;
-                for (int tile = rank; tile < I.n_tiles; tile += P) {
+                int nsx = 0;
+                if constexpr (ST) {
+                    stg.begin();
+                    const int o_x = stg.add(I.x, sizeof(T));
+                    const int o_dx = (final && I.dx) ? stg.add(I.dx, sizeof(T)) : -1;
+                    const int o_h = react ? stg.add(hout, sizeof(T)) : -1;
+                    const int o_fl = react ? stg.add(I.vflags, 1) : -1;
+                    const int nvs = min(k, stg.vec_cap());
+                    const int o_v = stg.lay_off;
+                    for (int i = 0; i < nvs; ++i) stg.add(Vb + (size_t)i * ldV, sizeof(T));
+                    nsx = stg.publish(rank, P, I.n_tiles);
+                    for (int tile = rank; nsx > 0 && tile < I.n_tiles; tile += P) {
+                        const unsigned char* sb = stg.acquire(abort_word);
+                        const T* xs = reinterpret_cast<const T*>(sb + o_x);
+                        double acc[VPT];
+#pragma unroll
+                        for (int v = 0; v < VPT; ++v) {
+                            const int li = v * kThreads + threadIdx.x;
+                            acc[v] = ((long long)tile * TILE + li < N) ? (double)xs[li] : 0.0;
+                        }
+                        for (int i0 = 0; i0 < k; i0 += kChunk) {
+                            T vv[kChunk][VPT];
+#pragma unroll
+                            for (int ii = 0; ii < kChunk; ++ii)
+#pragma unroll
+                                for (int v = 0; v < VPT; ++v) {
+                                    const int li = v * kThreads + threadIdx.x;
+                                    const long long n = (long long)tile * TILE + li;
+                                    const int i = i0 + ii;
+                                    T val = T(0);
+                                    if (i < k && n < N)
+                                        val = (i < nvs) ? reinterpret_cast<const T*>(sb + o_v + i * TILE * (int)sizeof(T))[li]
+                                                        : Vb[(size_t)i * ldV + n];
+                                    vv[ii][v] = val;
+                                }
+#pragma unroll
+                            for (int ii = 0; ii < kChunk; ++ii) {
+                                if (i0 + ii < k) {
+                                    const double cf = shc[i0 + ii];
+#pragma unroll
+                                    for (int v = 0; v < VPT; ++v) acc[v] += cf * (double)vv[ii][v];
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int v = 0; v < VPT; ++v) {
+                            const int li = v * kThreads + threadIdx.x;
+                            const long long n = (long long)tile * TILE + li;
+                            if (n < N) {
+                                if (final) {
+                                    I.u[n] = (T)acc[v];
+                                    if (o_dx >= 0) {
+                                        const double dxo = (double)reinterpret_cast<const T*>(sb + o_dx)[li];
+                                        I.dx[n] = (T)(dxo + (acc[v] - (double)xs[li]));
+                                    }
+                                } else {
+                                    I.x[n] = (T)acc[v];
+                                }
+                            }
+                        }
+                        if (react) {
+                            int32_t lt[VPT];
+#pragma unroll
+                            for (int v = 0; v < VPT; ++v) {
+                                const long long n = voxel(tile, v);
+                                lt[v] = (n < N && (T)acc[v] >= T(0.5)) ? I.lat[n] : 0;
+                            }
+#pragma unroll
+                            for (int v = 0; v < VPT; ++v) {
+                                const int li = v * kThreads + threadIdx.x;
+                                const long long n = (long long)tile * TILE + li;
+                                if (n < N)
+                                    react_voxel(n, (T)acc[v], reinterpret_cast<const T*>(sb + o_h)[li], lt[v], step, slot_now,
+                                                sb[o_fl + li], stim_next, hin);
+                            }
+                        }
+                        stg.release();
+                    }
+                }
+                for (int tile = rank; nsx == 0 && tile < I.n_tiles; tile += P) {
                     if (threadIdx.x < k) pf_slice(Vb + (size_t)threadIdx.x * ldV, sizeof(T), tile + P);
                     else if (threadIdx.x == k) pf_slice(I.x, sizeof(T), tile + P);
                     else if (threadIdx.x == k + 1 && final) pf_slice(I.dx, sizeof(T), tile + P);
@@ -1129,7 +1654,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     break;
                 }
                 // ============ true residual of the new iterate (start of the next cycle)
-                if (!team_sync(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
                     if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
                     else if (threadIdx.x == kRowArrays) pf_slice(I.x, sizeof(T), tile + P);
@@ -1143,7 +1668,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                             const bool rz = tb && (__ldg(I.vflags + n) & PHS_VFLAG_TBLOCK);
                             int32_t q[6];
                             T c[6];
-                            load_nb(I.nb, n, q);
+                            row_nb(n, q);
                             row_coef(I.coef, I.cw, I.m6, n, c);
                             T lap = rz ? T(0) : lap_row(I.x, xv, q, c);
                             if (EDGE && I.ecf && !rz) lap += edge_row(I.x, I.enb, I.ecf, n);
@@ -1160,7 +1685,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 }
                 groups_done(1);
                 mark(PF_CHECK);
-                if (!team_sync(I.sync, P, abort_word, ctl, leader_check)) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, leader_check)) { aborted = true; break; }
                 act = read_action();
                 mark(PF_CHECK_WAIT);
                 if (act == ACT_DONE) break;
@@ -1239,7 +1764,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         atomicExch(I.prof + PF_TEAM, (unsigned long long)P);
     }
     if (!aborted) {
-        if (!team_sync(I.sync, P, abort_word, ctl, [&]() {
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {
                 if (threadIdx.x == 0) {
                     I.st->step = step;
                     I.st->id_save = id_save;
@@ -1250,6 +1775,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
             aborted = true;
         }
     }
+    if constexpr (ST) stg.quit();   // the producer warp drains its copies and exits
 }
 
 // ------------------------------------------------------------------ fill kernel
@@ -1279,23 +1805,43 @@ constexpr int kVptF32Min = 2;    // the smallest voxels-per-thread of any FP32 v
 constexpr int kVptF64 = 1;
 
 // Compiled step-kernel variants: the same algorithm with different tile
-// lengths (voxels per thread; a tile is 256 x VPT consecutive voxels) and
-// register budgets (__launch_bounds__ minimum CTAs per SM).  The autotuner
-// picks one.  Each exists without and with the anisotropic edge terms.
+// lengths (voxels per thread; a tile is 256 x VPT consecutive voxels),
+// register budgets (__launch_bounds__ minimum CTAs per SM), neighbour tables
+// (int32 or compact) and, for the FP32 staged ones, the shared-memory ring of
+// the producer warp (bytes; sized so that MINB CTAs fit an SM next to the
+// kernel's static shared memory).  The autotuner picks one.  Each exists
+// without and with the anisotropic edge terms.
 using StepFnF = void (*)(const InstDev<float>*, const int4*, long long, unsigned int*);
 using StepFnD = void (*)(const InstDev<double>*, const int4*, long long, unsigned int*);
-const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2, false>, step_kernel<float, kVptF32, 3, false>,
-                            step_kernel<float, kVptF32, 4, false>, step_kernel<float, 2, 4, false>,
-                            step_kernel<float, 2, 5, false>};
-const StepFnF kStepF32Edge[] = {step_kernel<float, kVptF32, 2, true>, step_kernel<float, kVptF32, 3, true>,
-                                step_kernel<float, kVptF32, 4, true>, step_kernel<float, 2, 4, true>,
-                                step_kernel<float, 2, 5, true>};
-const int kMinbF32[] = {2, 3, 4, 4, 5};
-const int kVptOfF32[] = {kVptF32, kVptF32, kVptF32, 2, 2};
-const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2, false>, step_kernel<double, kVptF64, 3, false>};
-const StepFnD kStepF64Edge[] = {step_kernel<double, kVptF64, 2, true>, step_kernel<double, kVptF64, 3, true>};
+constexpr int kRing3 = 56 * 1024, kRing2 = 88 * 1024;
+const StepFnF kStepF32[] = {step_kernel<float, kVptF32, 2, false, 0, false>, step_kernel<float, kVptF32, 3, false, 0, false>,
+                            step_kernel<float, kVptF32, 4, false, 0, false>, step_kernel<float, 2, 4, false, 0, false>,
+                            step_kernel<float, 2, 5, false, 0, false>,       step_kernel<float, 2, 3, false, kRing3, false>,
+                            step_kernel<float, 4, 2, false, kRing2, false>,  step_kernel<float, 2, 5, false, 0, true>,
+                            step_kernel<float, kVptF32, 4, false, 0, true>};
+const StepFnF kStepF32Edge[] = {step_kernel<float, kVptF32, 2, true, 0, false>, step_kernel<float, kVptF32, 3, true, 0, false>,
+                                step_kernel<float, kVptF32, 4, true, 0, false>, step_kernel<float, 2, 4, true, 0, false>,
+                                step_kernel<float, 2, 5, true, 0, false>,       step_kernel<float, 2, 3, true, kRing3, false>,
+                                step_kernel<float, 4, 2, true, kRing2, false>,  step_kernel<float, 2, 5, true, 0, true>,
+                                step_kernel<float, kVptF32, 4, true, 0, true>};
+const int kMinbF32[] = {2, 3, 4, 4, 5, 3, 2, 5, 4};
+const int kVptOfF32[] = {kVptF32, kVptF32, kVptF32, 2, 2, 2, 4, 2, kVptF32};
+const int kRingF32[] = {0, 0, 0, 0, 0, kRing3, kRing2, 0, 0};
+// variants that read the compact neighbour table of every instance, and their
+// int32-table twin (launched instead when an unfinished instance has none)
+const int kTwinF32[] = {-1, -1, -1, -1, -1, -1, -1, 4, 2};
+const StepFnD kStepF64[] = {step_kernel<double, kVptF64, 2, false, 0, false>, step_kernel<double, kVptF64, 3, false, 0, false>};
+const StepFnD kStepF64Edge[] = {step_kernel<double, kVptF64, 2, true, 0, false>,
+                                step_kernel<double, kVptF64, 3, true, 0, false>};
 const int kMinbF64[] = {2, 3};
-constexpr int kNumF32 = 5, kNumF64 = 2;
+constexpr int kNumF32 = 9, kNumF64 = 2;
+// Threads per CTA and dynamic shared memory of a variant's launch.
+int ring_of(int prec_bytes, int variant) { return prec_bytes == 8 ? 0 : kRingF32[variant]; }
+int threads_of(int prec_bytes, int variant) { return kThreads + (ring_of(prec_bytes, variant) > 0 ? 32 : 0); }
+int dyn_smem_of(int prec_bytes, int variant) {
+    const int r = ring_of(prec_bytes, variant);
+    return r > 0 ? kRingHeader + r : 0;
+}
 
 // Tiles of an instance of n voxels under a variant.
 int tiles_of(long long n, int vpt) { return (int)((n + (long long)kThreads * vpt - 1) / ((long long)kThreads * vpt)); }
@@ -1405,7 +1951,13 @@ namespace {
 
 template <typename T>
 int occupancy_for(int* ctas, int variant, bool edge = false) {
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, step_fn<T>(variant, edge), kThreads, 0);
+    const void* fn = step_fn<T>(variant, edge);
+    const int smem = dyn_smem_of((int)sizeof(T), variant);
+    if (smem > 0) {
+        cudaError_t a = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (a != cudaSuccess) { set_last_error("ring shared memory", a); return PHS_ERR_CUDA; }
+    }
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, threads_of((int)sizeof(T), variant), smem);
     if (e != cudaSuccess) { set_last_error("occupancy", e); return PHS_ERR_CUDA; }
     return PHS_OK;
 }
@@ -1857,10 +2409,19 @@ std::vector<int> team_sizes(const std::vector<int>& tiles, const std::vector<dou
     return P;
 }
 
+// The variant a launch uses: the configured one, or its int32-table twin when
+// it reads compact tables and an unfinished instance has none (or the engine's
+// compact tables are off).
 template <typename T>
 int variant_of(const phs_engine* e) {
-    if (e->variant >= 0) return e->variant;
-    return sizeof(T) == 8 ? kDefaultF64 : kDefaultF32;
+    int v = e->variant >= 0 ? e->variant : (sizeof(T) == 8 ? kDefaultF64 : kDefaultF32);
+    if (sizeof(T) == 4 && kTwinF32[v] >= 0) {
+        bool all = e->compact_nb;
+        for (const auto& h : e->inst)
+            if (h.used && !h.finished && !h.nbr) all = false;
+        if (!all) v = kTwinF32[v];
+    }
+    return v;
 }
 
 void drop_graphs(phs_engine* e) {
@@ -1873,8 +2434,9 @@ cudaError_t launch_waves(phs_engine* e, long long n_steps, cudaStream_t stream) 
     for (auto& wv : e->waves) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)wv.second);
-        cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = 0;
+        const int variant = variant_of<T>(e);
+        cfg.blockDim = dim3((unsigned)threads_of((int)sizeof(T), variant));
+        cfg.dynamicSmemBytes = (size_t)dyn_smem_of((int)sizeof(T), variant);
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
@@ -1886,7 +2448,7 @@ cudaError_t launch_waves(phs_engine* e, long long n_steps, cudaStream_t stream) 
         long long ns = n_steps;
         unsigned int* ab = e->abort_word;
         void* args[] = {(void*)&dd, (void*)&mp, (void*)&ns, (void*)&ab};
-        cudaError_t ce = cudaLaunchKernelExC(&cfg, step_fn<T>(variant_of<T>(e), e->plan_edge), args);
+        cudaError_t ce = cudaLaunchKernelExC(&cfg, step_fn<T>(variant, e->plan_edge), args);
         if (ce != cudaSuccess) return ce;
     }
     return cudaSuccess;
@@ -2263,6 +2825,19 @@ int phs_step_variant_vpt(int precision, int32_t count, int32_t* vpt) {
     const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
     if (count < nv || !vpt) return PHS_ERR_BAD_ARG;
     for (int v = 0; v < nv; ++v) vpt[v] = precision == PHS_PREC_F64 ? kVptF64 : kVptOfF32[v];
+    return PHS_OK;
+}
+
+int phs_step_variant_layout(int precision, int32_t count, int32_t* ring_bytes, int32_t* compact_table) {
+    if (precision != PHS_PREC_F32 && precision != PHS_PREC_F64) return PHS_ERR_BAD_ARG;
+    const int nv = precision == PHS_PREC_F64 ? kNumF64 : kNumF32;
+    if (count < nv) return PHS_ERR_BAD_ARG;
+    for (int v = 0; v < nv; ++v) {
+        const bool f32 = precision == PHS_PREC_F32;
+        if (ring_bytes) ring_bytes[v] = f32 ? kRingF32[v] : 0;
+        // staged variants read the compact table of every instance that has one
+        if (compact_table) compact_table[v] = (f32 && (kTwinF32[v] >= 0 || kRingF32[v] > 0)) ? 1 : 0;
+    }
     return PHS_OK;
 }
 

@@ -274,6 +274,18 @@ class BatchedEngine:
             pass
 
 
+def step_variant_layout(precision=_lib.PREC_F32):
+    """[(ring bytes, reads the compact table)] per step-kernel variant: ring
+    bytes > 0 for the staged variants (producer warp, bulk copies into a
+    shared-memory ring)."""
+    n = len(step_variants(precision))
+    ring = np.zeros(n, dtype=np.int32)
+    comp = np.zeros(n, dtype=np.int32)
+    _lib.check(_lib.lib().phs_step_variant_layout(precision, n, _lib.ptr(ring, ctypes.c_int32),
+                                                  _lib.ptr(comp, ctypes.c_int32)), "phs_step_variant_layout")
+    return [(int(r), bool(c)) for r, c in zip(ring, comp)]
+
+
 def step_variants(precision=_lib.PREC_F32, with_vpt=False):
     """[(variant, min CTAs/SM it was compiled for, registers per thread)], with
     the voxels per thread (tile = 256 x VPT voxels) as a fourth entry when

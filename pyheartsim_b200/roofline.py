@@ -24,6 +24,11 @@ The plain form (GMRES(50) full cycles) also runs the true-residual test at the
 end of every cycle: read x, b, nb, coefficients; write V0 and u = 4 s + 24 + cb
 per cycle.
 
+The neighbour table costs nb = 24 bytes per row as six int32 indices, or 8
+with the compact table (four int16 offsets; the +-x neighbours follow from the
+row order, and the per-512-voxel base offsets add 1/32 byte per row): every
+"24" above becomes nb.
+
 Anisotropic rows (edge cross terms) add the edge table, 12 int32 indices and
 six coefficients = 48 + 6 s, to every operator application (the RHS stencil
 and each A_j): in FP32 +72 bytes per step and +72 per Arnoldi step.
@@ -34,8 +39,11 @@ def coef_bytes(s, iso):
     return (s + 1) if iso else 6 * s
 
 
-def bytes_rhs(s, cb):
-    return 8 * s + 26 + cb
+COMPACT_NB = 8 + 16 / 512
+
+
+def bytes_rhs(s, cb, nb=24):
+    return 8 * s + 2 + nb + cb
 
 
 def edge_bytes(s):
@@ -43,15 +51,15 @@ def edge_bytes(s):
 
 
 def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, guess=False, edge=False,
-                      checks=0):
+                      checks=0, nb=24):
     """Total algorithmic bytes of ``steps`` steps of an instance with ``voxels``
     voxels whose solves took ``k_sum`` Arnoldi steps in total (``k_sq_sum`` =
     sum of squares).  Steps that needed no iteration still run the RHS phase
     and the final copy (2 s).  ``checks``: true-residual tests at cycle ends
-    (full cycles)."""
+    (full cycles); ``nb``: neighbour-table bytes per row (24, or COMPACT_NB)."""
     cb = coef_bytes(s, iso)
-    per_voxel = (steps * (bytes_rhs(s, cb) + 2 * s) + (5 * s + 24 + cb) * k_sum + s * (k_sq_sum - k_sum)
-                 + s * k_sum + checks * (4 * s + 24 + cb))
+    per_voxel = (steps * (bytes_rhs(s, cb, nb) + 2 * s) + (5 * s + nb + cb) * k_sum + s * (k_sq_sum - k_sum)
+                 + s * k_sum + checks * (4 * s + nb + cb))
     if guess:     # read the increment in the RHS phase; read and rewrite it in the final update
         per_voxel += steps * s + 2 * s * (solves or 0)
     if edge:
@@ -59,5 +67,5 @@ def algorithmic_bytes(s, voxels, steps, k_sum, k_sq_sum, solves=None, iso=True, 
     return voxels * per_voxel
 
 
-def per_voxel_step(s, k, iso=True):
-    return algorithmic_bytes(s, 1, 1, k, k * k, iso=iso)
+def per_voxel_step(s, k, iso=True, nb=24):
+    return algorithmic_bytes(s, 1, 1, k, k * k, iso=iso, nb=nb)
