@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--c2-walls", type=int, nargs="*", default=[3, 8], help="wall thicknesses of the c2 runs")
     p.add_argument("--accuracy-only", action="store_true", help="run only the accuracy leg")
     p.add_argument("--no-tune", action="store_true", help="use the default step-kernel variant")
+    p.add_argument("--variant", type=int, default=None,
+                   help="run this step-kernel variant (with --ctas-per-sm) instead of tuning (profiling cases)")
+    p.add_argument("--ctas-per-sm", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--serving-requests", type=int, default=300)
     p.add_argument("--egm-nv", type=int, default=500_000)
@@ -201,16 +204,28 @@ def run_b200(args):
         return [S] * (count // S) + ([count % S] if count % S else [])
     stream = torch.cuda.current_stream(dev)
 
+    pre = (args.pre_steps // S) * S
+    tune = None
+    if args.variant is not None:
+        tune = {"best": (args.variant, args.ctas_per_sm), "fixed": True}
+    elif not args.no_tune:
+        # tuned on a copy of the batch advanced to the timed window's start, so
+        # the options are compared mid-propagation and the timed run below
+        # covers the same simulated steps whatever the number of options
+        from pyheartsim_b200 import autotune
+        eng_t = BatchedEngine(_lib.PREC_F32)
+        for x in insts:
+            eng_t.add(x)
+        for _ in range(pre // S):
+            eng_t.advance(S, stream=stream, sync=False)
+        tune = autotune.tune(eng_t, steps=S, stream=stream)
+        eng_t.close()
     eng = BatchedEngine(_lib.PREC_F32)
     slots = [eng.add(x) for x in insts]
     for x in insts:
         x.release_tables()
-    pre = (args.pre_steps // S) * S
-    tune = None
-    if not args.no_tune:
-        from pyheartsim_b200 import autotune
-        tune = autotune.tune(eng, steps=S, stream=stream)
-        pre = max(0, pre - S * 2 * len(tune.get("table", [])))
+    if tune is not None:
+        eng.configure(variant=tune["best"][0], ctas_per_sm=tune["best"][1])
     # team sizes from each instance's measured cost: the last BALANCE_LAUNCHES x
     # 3 launches of the (untimed) pre-steps run with the phase timers on, in
     # three rounds that each re-split the CTAs by the cost measured in the
