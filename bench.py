@@ -30,11 +30,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99 latency"
+DEFAULT_F32_VARIANT = 2        # the engine's FP32 default when the autotuner is off
 # DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of the two timed full-size launches of this batch, 2.71
 # Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md);
 # multiplied by the voxels and steps of one launch below.
-DEFAULT_F32_VARIANT = 2        # the engine's FP32 default when the autotuner is off
 STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 267.0
 STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.71
 BALANCE_LAUNCHES = 10   # launches per team-balancing round in the pre-steps
