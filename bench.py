@@ -33,9 +33,10 @@ METRIC = "voxel-steps/s batched FP32 vs plain FP64 on 1 B200 at LAT err<=dt; p99
 DEFAULT_F32_VARIANT = 2        # the engine's FP32 default when the autotuner is off
 # DRAM bytes per voxel-step of step_kernel measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of the two timed full-size launches of this batch, 2.71
-# Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md);
-# multiplied by the voxels and steps of one launch below.
-STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = 267.0
+# Arnoldi steps per step, profiles/step_kernel_64shells_dram_fullsize.md), for
+# the variants that read the int32 neighbour table and those that read the
+# compact one; multiplied by the voxels and steps of one launch below.
+STEP_TRAFFIC_BYTES_PER_VOXEL_STEP = {"int32": 267.0, "compact": 201.0}
 STEP_TRAFFIC_ARNOLDI_PER_STEP = 2.71
 BALANCE_LAUNCHES = 10   # launches per team-balancing round in the pre-steps
 WORKLOAD = "64 shells, 50k-400k voxels log-uniform, scar 0-30%, focal pacing, MS+AP, FP32 state / FP64 dots"
@@ -312,7 +313,8 @@ def run_b200(args):
                        "arnoldi_per_step": float(k_sum.sum() / (K * len(ns)))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
-                         "traffic": STEP_TRAFFIC_BYTES_PER_VOXEL_STEP * float(ns.sum()) * S,
+                         "traffic": STEP_TRAFFIC_BYTES_PER_VOXEL_STEP["compact" if reads_compact else "int32"]
+                         * float(ns.sum()) * S,
                          "traffic_source": ("ncu dram__bytes_read+write per voxel-step of full-size launches of this "
                                             f"batch ({STEP_TRAFFIC_ARNOLDI_PER_STEP} Arnoldi steps per step) x voxels "
                                             "x steps per launch"),
