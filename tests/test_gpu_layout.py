@@ -93,8 +93,8 @@ def _run_batch(insts, **cfg):
 @pytest.mark.parametrize("fast", [True, False])
 def test_staged_and_compact_variants_same_history(fast, cuda_device):
     """The staged kernels (bulk copies into a shared-memory ring) and the
-    compact-table kernels compute what the int32-table kernel does, bit for
-    bit: early exit and full GMRES cycles, isotropic and anisotropic rows,
+    compact-table kernels compute what the int32-table kernel of the same tile
+    length does, bit for bit: early exit and full GMRES cycles, isotropic and anisotropic rows,
     compact and int32 neighbour tables (a compact variant with the tables off
     runs its int32 twin), one and several CTAs per SM."""
     from pyheartsim_b200.engine import step_variant_layout, step_variants
@@ -102,8 +102,12 @@ def test_staged_and_compact_variants_same_history(fast, cuda_device):
     lay = step_variant_layout(_lib.PREC_F32)
     assert all(lay[v][0] > 0 for v in STAGED) and all(lay[v] == (0, True) for v in COMPACT)
     insts = _batch(fast)
-    ref = _run_batch(insts, variant=2)
+    # partial sums are grouped by tile, so each variant is compared with the
+    # int32-table variant of its tile length (512 voxels: 4, 1024: 2)
+    vpt = {v: t for v, _, _, t in step_variants(_lib.PREC_F32, with_vpt=True)}
+    refs = {vpt[4]: _run_batch(insts, variant=4), vpt[2]: _run_batch(insts, variant=2)}
     for var in STAGED + COMPACT:
+        ref = refs[vpt[var]]
         for cps, compact in ((1, True), (0, True), (1, False)):
             got = _run_batch(insts, variant=var, ctas_per_sm=cps, compact_nb=compact)
             for (h0, i0), (h1, i1) in zip(ref, got):
