@@ -2,8 +2,9 @@
 
 Times every compiled step-kernel variant (voxels per thread, i.e. the tile
 length of 256 x VPT voxels, and register budget) at every feasible
-CTAs-per-SM setting on the engine's live instances, keeps the fastest and
-leaves the engine configured with it.  Each option is timed ``repeats`` times
+CTAs-per-SM setting on the engine's live instances, keeps the fastest (the
+first option within 1 % of the fastest median, so near-ties resolve the same
+way every run) and leaves the engine configured with it.  Each option is timed ``repeats`` times
 (one launch of ``steps`` steps each, after a warm launch that also captures
 its graph) and ranked by the median.  Tuning advances the instances like any
 other call (the steps are real work).
@@ -26,6 +27,7 @@ from . import _lib
 from .engine import step_variants
 
 _CACHE = {}
+TIE_FRAC = 0.01
 
 
 def cache_path():
@@ -95,7 +97,11 @@ def tune(engine, steps=10, stream=None, cps_options=None, repeats=5, use_file=Tr
             table.append({"variant": variant, "voxels_per_thread": vpt, "min_ctas": minb, "regs": regs,
                           "ctas_per_sm": cps, "ms_per_step": times[len(times) // 2],
                           "ms_per_step_min": times[0], "ms_per_step_max": times[-1]})
-    best = min(table, key=lambda r: r["ms_per_step"])
+    # the first option (variant, then CTAs per SM, ascending) within TIE_FRAC
+    # of the fastest median: options that differ by less than the run-to-run
+    # spread do not flip the choice between runs
+    fastest = min(r["ms_per_step"] for r in table)
+    best = next(r for r in table if r["ms_per_step"] <= fastest * (1.0 + TIE_FRAC))
     _CACHE[key] = (best["variant"], best["ctas_per_sm"])
     if use_file:
         _store_file(key, _CACHE[key])
