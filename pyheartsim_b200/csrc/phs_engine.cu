@@ -414,9 +414,18 @@ struct SharedCtl {
 // Bounded team barrier.  The last CTA to arrive runs `leader` (whole CTA)
 // before releasing the others.  Returns false when the wait gave up or another
 // team aborted; the kernel then leaves all loops.
+//
+// The release word carries, besides a barrier counter (bits 9-31), the
+// action (bits 0-2) and cycle length k (bits 3-8) the leader left in `sc`, so
+// the waiting CTAs learn them from the load that releases them (ctl.action,
+// ctl.k).  Ordering: the arrival is an acq_rel RMW (the CTA's writes, made
+// visible to thread 0 by the CTA barrier and the fence, precede it; the
+// leader's RMW acquires every earlier arrival); the release is a release store
+// and the waiters' polls are acquire loads.
+constexpr unsigned int kGenShift = 9;
 template <bool ST, typename Leader>
 __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abort_word, SharedCtl& ctl,
-                                          Leader&& leader) {
+                                          const Scalars* sc, Leader&& leader) {
     csync<ST>();
     if (threadIdx.x == 0) {
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
@@ -427,7 +436,6 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
         ctl.last = (a == (unsigned int)(P - 1));
         ctl.gen = g;
         ctl.abort = 0;
-        if (ctl.last) __threadfence();
     }
     csync<ST>();
     if (ctl.last) {
@@ -436,16 +444,21 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
         if (threadIdx.x == 0) {
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(ts->count);
+            const int act = __ldcg(&sc->action), k = __ldcg(&sc->k);
+            ctl.action = act;
+            ctl.k = k;
             cnt.store(0u, cuda::memory_order_relaxed);
-            __threadfence();
-            gen.store(ctl.gen + 1u, cuda::memory_order_release);
+            const unsigned int word = ((((ctl.gen >> kGenShift) + 1u) << kGenShift)) | ((unsigned int)(k & 63) << 3) |
+                                      (unsigned int)(act & 7);
+            gen.store(word, cuda::memory_order_release);
         }
     } else if (threadIdx.x == 0) {
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ab(*abort_word);
         unsigned long long t0 = global_ns();
         unsigned int polls = 0;
-        while (gen.load(cuda::memory_order_acquire) == ctl.gen) {
+        unsigned int word;
+        while ((word = gen.load(cuda::memory_order_acquire)) == ctl.gen) {
             if (ab.load(cuda::memory_order_relaxed) != 0u) { ctl.abort = 1; break; }
             if (++polls > kWaitPolls || global_ns() - t0 > kWaitNs) {
                 ab.fetch_or(1u, cuda::memory_order_relaxed);
@@ -454,7 +467,8 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
             }
             __nanosleep(64);
         }
-        __threadfence();
+        ctl.action = (int)(word & 7u);
+        ctl.k = (int)((word >> 3) & 63u);
     }
     csync<ST>();
     return ctl.abort == 0;
@@ -1035,14 +1049,8 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
 
-    auto read_action = [&]() {
-        if (threadIdx.x == 0) {
-            ctl.action = __ldcg(&sc->action);
-            ctl.k = __ldcg(&sc->k);
-        }
-        csync<ST>();
-        return ctl.action;
-    };
+    // the action and cycle length of the barrier that just ended (team_sync)
+    auto read_action = [&]() { return ctl.action; };
 
     auto load_shc = [&](int cnt) {
         csync<ST>();
@@ -1165,7 +1173,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         pending = -1;
         mark(PF_RHS1);
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {})) { aborted = true; break; }
         mark(PF_RHS_WAIT);
         int nst = 0;
         if constexpr (ST) {
@@ -1270,7 +1278,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         groups_done(2);
         mark(PF_RHS);
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, leader_rhs)) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, leader_rhs)) { aborted = true; break; }
         int act = read_action();
         mark(PF_RHS_WAIT);
         // end of this step: its history slot, and whether the pass that writes
@@ -1406,7 +1414,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(j + 1);
                     mark(PF_A);
-                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() { leader_dots(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() { leader_dots(j); })) { aborted = true; break; }
                     load_shc(j + 1);
                     mark(PF_A_WAIT);
                     // ============ phase C: u = w - sum_i c_i V_i  (in place), ||u||^2
@@ -1510,7 +1518,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(1);
                     mark(PF_C);
-                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() { leader_norm(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() { leader_norm(j); })) { aborted = true; break; }
                     act = read_action();
                     mark(PF_C_WAIT);
                     if (prof_on && threadIdx.x == 0) pf[PF_SOLVE_ITERS] += 1;
@@ -1654,7 +1662,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     break;
                 }
                 // ============ true residual of the new iterate (start of the next cycle)
-                if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {})) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {})) { aborted = true; break; }
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
                     if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
                     else if (threadIdx.x == kRowArrays) pf_slice(I.x, sizeof(T), tile + P);
@@ -1685,7 +1693,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 }
                 groups_done(1);
                 mark(PF_CHECK);
-                if (!team_sync<ST>(I.sync, P, abort_word, ctl, leader_check)) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, leader_check)) { aborted = true; break; }
                 act = read_action();
                 mark(PF_CHECK_WAIT);
                 if (act == ACT_DONE) break;
@@ -1764,7 +1772,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         atomicExch(I.prof + PF_TEAM, (unsigned long long)P);
     }
     if (!aborted) {
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, [&]() {
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {
                 if (threadIdx.x == 0) {
                     I.st->step = step;
                     I.st->id_save = id_save;
