@@ -382,6 +382,10 @@ def phase_profile(eng, slots, S, stream):
         st = max(p.pop("steps"), 1)
         it = p.pop("arnoldi_iters")
         team = p.pop("team_ctas")
+        lead = p.pop("leader", 0.0)          # leader bodies, on the team's critical path
+        nbar = p.pop("barriers", 0)
+        acc["leader"] = acc.get("leader", 0.0) + lead / st
+        acc["barriers_per_step"] = acc.get("barriers_per_step", 0.0) + nbar / st
         inst = eng.instance(s)
         per.append([int(inst.n_voxel), int(inst.model), int(team), round(it / st, 2),
                     round(sum(p.values()) / st, 4), round(p["rhs_reaction"] / st, 4), round(p["rhs"] / st, 4)])
@@ -526,6 +530,7 @@ def plain_leg(args, cases, fast_value, dev):
     st = max(prof.pop("steps"), 1)
     prof.pop("team_ctas", None)
     it = prof.pop("arnoldi_iters")
+    nbar = prof.pop("barriers", 0)
     pk, pk_src = peaks()
     achieved = alg / (ms / 1e3) / 1e9
     v = meta["n"] * steps / (ms / 1e3)
@@ -535,7 +540,8 @@ def plain_leg(args, cases, fast_value, dev):
                          "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
                          "bytes_per_voxel_step": alg / (meta["n"] * steps),
                          "note": "the 51-column FP64 Krylov basis of this instance fits in L2"},
-            "phases_ms_per_step": {k: round(v_ / st, 4) for k, v_ in prof.items()},
+            "phases_ms_per_step": {**{k: round(v_ / st, 4) for k, v_ in prof.items()},
+                                   "barriers_per_step": round(nbar / st, 2)},
             "speedup_batched_fp32": fast_value / v}
 
 

@@ -198,7 +198,9 @@ int phs_engine_rebalance(phs_engine* eng);
  * residual), [1] the RHS barriers, [2] Arnoldi phase A, [3] its barrier, [4]
  * phase C, [5] its barrier, [6] update, [7] residual check, [8] its barrier,
  * [9] final copy, [10] RHS pass 1 (reaction); [11] steps and
- * [12] Arnoldi iterations counted; [13] CTAs in the team at the last launch.   */
+ * [12] Arnoldi iterations counted; [13] CTAs in the team at the last launch;
+ * [14] nanoseconds in the leader bodies of the team's barriers (whichever CTA
+ * led) and [15] team barriers passed.                                          */
 int phs_instance_profile(phs_engine* eng, int slot, uint64_t* out16);
 /* Bytes per voxel of the neighbour table the instance's compact-table variants
  * read: 8 (compact form, PHS_CFG_COMPACT_NB) or 24 (int32 table).              */

@@ -38,7 +38,7 @@ CFG_WAVE_INSTANCES = 6
 CFG_GROUP_SUMS = 7
 CFG_COMPACT_NB = 9
 PROFILE_SLOTS = ("rhs", "rhs_wait", "arnoldi_a", "arnoldi_a_wait", "arnoldi_c", "arnoldi_c_wait", "update",
-                 "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas")
+                 "check", "check_wait", "copy", "rhs_reaction", "steps", "arnoldi_iters", "team_ctas", "leader", "barriers")
 
 VFLAG_S1 = 1
 VFLAG_S2 = 2

@@ -63,7 +63,10 @@ enum Phase : int { PH_PLAIN = 0, PH_RHS = 1, PH_DOTS = 2, PH_NORM = 3, PH_CHECK 
 // Phase timer slots (nanoseconds of globaltimer, summed over steps).
 enum ProfSlot : int {
     PF_RHS = 0, PF_RHS_WAIT, PF_A, PF_A_WAIT, PF_C, PF_C_WAIT, PF_X, PF_CHECK, PF_CHECK_WAIT,
-    PF_COPY, PF_RHS1, PF_STEPS, PF_SOLVE_ITERS, PF_TEAM, kProfSlots = 16
+    PF_COPY, PF_RHS1, PF_STEPS, PF_SOLVE_ITERS, PF_TEAM,
+    PF_LEADER,      // time in the leader bodies of the team's barriers (whichever CTA led)
+    PF_BARRIERS,    // team barriers passed
+    kProfSlots = 16
 };
 
 struct Scalars {
@@ -425,7 +428,7 @@ struct SharedCtl {
 constexpr unsigned int kGenShift = 9;
 template <bool ST, typename Leader>
 __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abort_word, SharedCtl& ctl,
-                                          const Scalars* sc, Leader&& leader) {
+                                          const Scalars* sc, unsigned long long* prof, Leader&& leader) {
     csync<ST>();
     if (threadIdx.x == 0) {
         cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
@@ -439,9 +442,14 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, int P, unsigned int* abo
     }
     csync<ST>();
     if (ctl.last) {
+        const unsigned long long tl = (prof && threadIdx.x == 0) ? global_ns() : 0ull;
         leader();
         csync<ST>();
         if (threadIdx.x == 0) {
+            if (prof) {
+                atomicAdd(prof + PF_LEADER, global_ns() - tl);
+                atomicAdd(prof + PF_BARRIERS, 1ull);
+            }
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ts->gen);
             cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(ts->count);
             const int act = __ldcg(&sc->action), k = __ldcg(&sc->k);
@@ -839,31 +847,49 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
     };
 
     // ---- leader bodies ------------------------------------------------------
-    // Deterministic sums of partial slots slot0 .. slot0+ns-1 over all tiles, by
-    // the whole leader CTA: thread t adds partials t, t+256, ... in order (four
-    // or eight slots per pass, their loads issued together), then a fixed xor tree per
-    // warp and the warp results in warp order.  The order depends only on the
-    // partial count, not on the team size.  Results in bsum_out[0..ns).
+    // Deterministic sums of partial slots slot0 .. slot0+ns-1 over all partials,
+    // by the whole leader CTA; results in bsum_out[0..ns).  The order depends
+    // only on the partial count, not on the team size.
+    //  FP32 (a partial per tile and warp: many partials, few slots): thread t
+    //  adds partials t, t+256, ... in order, four slots per pass with their loads
+    //  issued together, then a fixed xor tree per warp.
+    //  FP64 (a partial per group of tiles: few partials, up to 51 slots in a
+    //  GMRES(50) cycle): lane l of warp w adds slot l (and l + 32) over partials
+    //  w, w+8, ... in order, its loads issued together, so one pass of loads
+    //  serves every slot.
+    //  Both end with the warp results added in warp order.
     __shared__ double bsum_w[kMaxRestart + 1][kWarps];
     __shared__ double bsum_out[kMaxRestart + 1];
-    // FP64 (one partial per tile, long GMRES(50) cycles): eight slots per pass
-    constexpr int kSumW = sizeof(T) == 8 ? 8 : 4;
+    constexpr int kSumW = 4;
     auto block_sum = [&](int slot0, int ns) {
-        for (int s0 = 0; s0 < ns; s0 += kSumW) {
-            double a[kSumW];
+        if constexpr (kWarpParts<T>) {
+            for (int s0 = 0; s0 < ns; s0 += kSumW) {
+                double a[kSumW];
 #pragma unroll
-            for (int u = 0; u < kSumW; ++u) a[u] = 0.0;
+                for (int u = 0; u < kSumW; ++u) a[u] = 0.0;
 #pragma unroll 4
-            for (int q = threadIdx.x; q < nparts; q += kThreads) {
-                const double* pq = psum + (size_t)q * ps + slot0 + s0;
+                for (int q = threadIdx.x; q < nparts; q += kThreads) {
+                    const double* pq = psum + (size_t)q * ps + slot0 + s0;
 #pragma unroll
-                for (int u = 0; u < kSumW; ++u)
-                    if (s0 + u < ns) a[u] += __ldcg(pq + u);
+                    for (int u = 0; u < kSumW; ++u)
+                        if (s0 + u < ns) a[u] += __ldcg(pq + u);
+                }
+#pragma unroll
+                for (int u = 0; u < kSumW; ++u) {
+                    const double v = warp_sum(a[u]);
+                    if (lane == 0 && s0 + u < ns) bsum_w[s0 + u][warp] = v;
+                }
             }
-#pragma unroll
-            for (int u = 0; u < kSumW; ++u) {
-                const double v = warp_sum(a[u]);
-                if (lane == 0 && s0 + u < ns) bsum_w[s0 + u][warp] = v;
+        } else {
+            for (int s0 = 0; s0 < ns; s0 += 32) {
+                const int sl = s0 + lane;
+                if (sl < ns) {
+                    const double* pq = psum + slot0 + sl;
+                    double a = 0.0;
+#pragma unroll 8
+                    for (int q = warp; q < nparts; q += kWarps) a += __ldcg(pq + (size_t)q * ps);
+                    bsum_w[sl][warp] = a;
+                }
             }
         }
         csync<ST>();
@@ -1173,7 +1199,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         pending = -1;
         mark(PF_RHS1);
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {})) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, [&]() {})) { aborted = true; break; }
         mark(PF_RHS_WAIT);
         int nst = 0;
         if constexpr (ST) {
@@ -1278,7 +1304,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         }
         groups_done(2);
         mark(PF_RHS);
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, leader_rhs)) { aborted = true; break; }
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, leader_rhs)) { aborted = true; break; }
         int act = read_action();
         mark(PF_RHS_WAIT);
         // end of this step: its history slot, and whether the pass that writes
@@ -1414,7 +1440,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(j + 1);
                     mark(PF_A);
-                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() { leader_dots(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, [&]() { leader_dots(j); })) { aborted = true; break; }
                     load_shc(j + 1);
                     mark(PF_A_WAIT);
                     // ============ phase C: u = w - sum_i c_i V_i  (in place), ||u||^2
@@ -1518,7 +1544,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     }
                     groups_done(1);
                     mark(PF_C);
-                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() { leader_norm(j); })) { aborted = true; break; }
+                    if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, [&]() { leader_norm(j); })) { aborted = true; break; }
                     act = read_action();
                     mark(PF_C_WAIT);
                     if (prof_on && threadIdx.x == 0) pf[PF_SOLVE_ITERS] += 1;
@@ -1662,7 +1688,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                     break;
                 }
                 // ============ true residual of the new iterate (start of the next cycle)
-                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {})) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, [&]() {})) { aborted = true; break; }
                 for (int tile = rank; tile < I.n_tiles; tile += P) {
                     if (threadIdx.x < kRowArrays) pf_rows(threadIdx.x, tile + P);
                     else if (threadIdx.x == kRowArrays) pf_slice(I.x, sizeof(T), tile + P);
@@ -1693,7 +1719,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
                 }
                 groups_done(1);
                 mark(PF_CHECK);
-                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, leader_check)) { aborted = true; break; }
+                if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, leader_check)) { aborted = true; break; }
                 act = read_action();
                 mark(PF_CHECK_WAIT);
                 if (act == ACT_DONE) break;
@@ -1772,7 +1798,7 @@ step_kernel(const InstDev<T>* __restrict__ insts, const int4* __restrict__ cta_m
         atomicExch(I.prof + PF_TEAM, (unsigned long long)P);
     }
     if (!aborted) {
-        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, [&]() {
+        if (!team_sync<ST>(I.sync, P, abort_word, ctl, sc, I.prof, [&]() {
                 if (threadIdx.x == 0) {
                     I.st->step = step;
                     I.st->id_save = id_save;

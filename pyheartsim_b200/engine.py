@@ -242,7 +242,7 @@ class BatchedEngine:
         _lib.check(_lib.lib().phs_instance_profile(self._h, slot, out), "phs_instance_profile")
         d = {}
         for i, name in enumerate(_lib.PROFILE_SLOTS):
-            d[name] = int(out[i]) if name in ("steps", "arnoldi_iters", "team_ctas") else out[i] / 1e6
+            d[name] = int(out[i]) if name in ("steps", "arnoldi_iters", "team_ctas", "barriers") else out[i] / 1e6
         return d
 
     def table_bytes(self, slot):
