@@ -74,6 +74,7 @@ def parse():
     p.add_argument("--aniso-only", action="store_true", help="run only the anisotropic (fibre) leg")
     p.add_argument("--aniso-instances", type=int, default=16)
     p.add_argument("--geometry-only", action="store_true", help="run only the geometry-preparation leg")
+    p.add_argument("--plain-only", action="store_true", help="run only the plain-FP64 leg (profiling case)")
     return p.parse_args()
 
 
@@ -542,7 +543,7 @@ def plain_leg(args, cases, fast_value, dev):
                          "note": "the 51-column FP64 Krylov basis of this instance fits in L2"},
             "phases_ms_per_step": {**{k: round(v_ / st, 4) for k, v_ in prof.items()},
                                    "barriers_per_step": round(nbar / st, 2)},
-            "speedup_batched_fp32": fast_value / v}
+            "speedup_batched_fp32": (fast_value / v) if fast_value else None}
 
 
 def geometry_leg(args, dev, n_target=1_000_000, reps=3):
@@ -923,6 +924,14 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"accuracy": accuracy_leg(dev, args.tol, walls=tuple(args.c2_walls))}), flush=True)
+        return 0
+    if args.plain_only:
+        import torch
+        from pyheartsim_b200 import workloads
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        cases = workloads.batched_inputs(args.instances, args.n_min, args.n_max, args.seed, t_phys=args.t_phys)
+        print(json.dumps({"plain_fp64": plain_leg(args, cases, None, dev)}), flush=True)
         return 0
     if args.aniso_only:
         import torch
