@@ -75,6 +75,9 @@ def parse():
     p.add_argument("--aniso-instances", type=int, default=16)
     p.add_argument("--geometry-only", action="store_true", help="run only the geometry-preparation leg")
     p.add_argument("--plain-only", action="store_true", help="run only the plain-FP64 leg (profiling case)")
+    p.add_argument("--serving-only", action="store_true", help="run only the two serving legs")
+    p.add_argument("--serving-sync", action="store_true",
+                   help="retire served requests with a synchronous history download (comparison runs)")
     return p.parse_args()
 
 
@@ -738,7 +741,8 @@ def serving_leg(args, dev, count=300, compress=20.0, rate=20.0, dur_ms=(200.0, 2
     t_prep = time.perf_counter() - t_prep
     free = torch.cuda.mem_get_info(dev)[0]
     srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
-                         stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True)
+                         stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True,
+                         async_download=not args.serving_sync)
     done, totals = srv.run(reqs)
     srv.close()
     out = serving.summarize(done, totals, reqs)
@@ -748,6 +752,7 @@ def serving_leg(args, dev, count=300, compress=20.0, rate=20.0, dur_ms=(200.0, 2
     out["arrival_rate_per_s"] = r_eff
     out["durations_ms"] = list(d)
     out["time_compression"] = compress
+    out["history_download"] = "synchronous" if args.serving_sync else "worker thread, pinned staging, own stream"
     if plain_subset:
         by_id = {r.rid: r for r in done}
         sub = sorted(reqs, key=lambda r: r.arrival_s)[:plain_subset]
@@ -924,6 +929,13 @@ def main():
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"accuracy": accuracy_leg(dev, args.tol, walls=tuple(args.c2_walls))}), flush=True)
+        return 0
+    if args.serving_only:
+        import torch
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        out = {"serving": serving_leg(args, dev, count=args.serving_requests, plain_subset=0)}
+        print(json.dumps(out), flush=True)
         return 0
     if args.plain_only:
         import torch

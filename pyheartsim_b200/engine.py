@@ -13,6 +13,45 @@ import numpy as np
 from . import _lib
 
 
+def tensor_to_host(t, stage=None, stage_bytes=128 << 20, stream=None):
+    """Copy a 2-D CUDA tensor to a new numpy array through two pinned staging
+    buffers (reused when ``stage`` holds large enough ones of the same dtype),
+    on ``stream`` (default: a new stream of the tensor's device); each chunk's
+    device-to-host copy overlaps the host copy of the one before.  Returns
+    (array, staging buffers).  Safe to call from a worker thread."""
+    import torch
+    rows, n = t.shape
+    out = np.empty((rows, n), dtype=np.float32 if t.dtype == torch.float32 else np.float64)
+    if rows == 0:
+        return out, stage
+    dev = t.device
+    per = max(1, int(stage_bytes // max(1, n * t.element_size())))
+    if stage is None or stage[0].numel() < per * n or stage[0].dtype != t.dtype:
+        stage = [torch.empty(per * n, dtype=t.dtype, pin_memory=True) for _ in range(2)]
+    stream = stream or torch.cuda.Stream(dev)
+    events = [None, None]
+    prev = None
+    with torch.cuda.stream(stream):
+        for k, a in enumerate(range(0, rows, per)):
+            b = min(rows, a + per)
+            buf = stage[k % 2]
+            if events[k % 2] is not None:
+                events[k % 2].synchronize()          # its previous chunk has been copied out below
+            buf[:(b - a) * n].view(b - a, n).copy_(t[a:b], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            if prev is not None:
+                pa, pb, pbuf, pev = prev
+                pev.synchronize()
+                np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
+            prev = (a, b, buf, ev)
+            events[k % 2] = ev
+        pa, pb, pbuf, pev = prev
+        pev.synchronize()
+        np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
+    return out, stage
+
+
 class BatchedEngine:
     def __init__(self, precision=_lib.PREC_F32):
         self.precision = precision
@@ -123,39 +162,9 @@ class BatchedEngine:
         the host through two reused pinned staging buffers of ``stage_bytes``
         (each chunk's device-to-host copy overlaps the host copy of the one
         before).  Same values as :meth:`history`."""
-        import torch
         t = self.history_device(slot, s0, count)
-        rows, n = t.shape
-        out = np.empty((rows, n), dtype=_lib.np_dtype(self.precision))
-        if rows == 0:
-            return out
-        dev = t.device
-        per = max(1, int(stage_bytes // max(1, n * t.element_size())))
         st = getattr(self, "_stage", None)
-        if st is None or st[0].numel() < per * n or st[0].dtype != t.dtype:
-            st = [torch.empty(per * n, dtype=t.dtype, pin_memory=True) for _ in range(2)]
-            self._stage = st
-        stream = torch.cuda.Stream(dev)
-        events = [None, None]
-        prev = None
-        with torch.cuda.stream(stream):
-            for k, a in enumerate(range(0, rows, per)):
-                b = min(rows, a + per)
-                buf = st[k % 2]
-                if events[k % 2] is not None:
-                    events[k % 2].synchronize()          # its previous chunk has been copied out below
-                buf[:(b - a) * n].view(b - a, n).copy_(t[a:b], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(stream)
-                if prev is not None:
-                    pa, pb, pbuf, pev = prev
-                    pev.synchronize()
-                    np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
-                prev = (a, b, buf, ev)
-                events[k % 2] = ev
-            pa, pb, pbuf, pev = prev
-            pev.synchronize()
-            np.copyto(out[pa:pb], pbuf[:(pb - pa) * n].numpy().reshape(pb - pa, n))
+        out, self._stage = tensor_to_host(t, st, stage_bytes)
         return out
 
     def activation_times(self, slot, max_per_voxel=16, threshold=0.5, stream=None):

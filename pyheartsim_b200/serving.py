@@ -12,10 +12,10 @@ between launches,
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
 * retires instances that reached their last step: gathers the whole 1 kHz Vm
-  history into the caller's voxel order on the device, copies it to the host
-  (a request's latency ends when its history is there) and frees the
-  instance.  (Copying on worker threads while the engine ran on was measured
-  slower: large pageable copies stall the main thread's launches.);
+  history into the caller's voxel order on the device, frees the instance and
+  copies the history to the host on a worker thread through pinned staging
+  buffers on its own stream while the engine keeps running
+  (``async_download``; a request's latency ends when its history is there);
 * re-splits CTAs over the running instances by measured cost every
   ``rebalance_every`` launches (the device phase timers run only in the launch
   before each re-split).
@@ -145,7 +145,8 @@ class _Inline:
 
 class Server:
     def __init__(self, hbm_budget_bytes, steps_per_launch=50, rebalance_every=8, build_threads=8, tol=1e-7,
-                 stream=None, engine=None, builder=None, footprint=None, device_build=False, max_active=64):
+                 stream=None, engine=None, builder=None, footprint=None, device_build=False, max_active=64,
+                 async_download=True):
         self.budget = int(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.S = int(steps_per_launch)
@@ -158,6 +159,12 @@ class Server:
             engine.configure(auto_balance=False)      # the server re-splits the CTAs itself
         self.engine = engine
         self.pool = ThreadPoolExecutor(max_workers=build_threads) if build_threads > 0 else _Inline()
+        # retired histories: gathered on the device, the instance freed, and the
+        # copy to the host made on this worker while the engine keeps running
+        self.async_download = bool(async_download) and hasattr(self.engine, "history_device")
+        self.dl = ThreadPoolExecutor(max_workers=1) if self.async_download else None
+        self._dl_tls = threading.local()
+        self._used_lock = threading.Lock()
         self.stream = stream
         self.used = 0
         self.launches = 0
@@ -175,6 +182,7 @@ class Server:
         nxt = 0
         work = 0.0
         dev_dl = hasattr(self.engine, "history_host")
+        downloading = []
         while nxt < len(reqs) or queue or active:
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival_s * time_scale <= now:
@@ -187,7 +195,9 @@ class Server:
                     break                                  # head still compiling; keep the GPU busy
                 inst = r.future.result()
                 fp = self.footprint(inst)
-                if active and (self.used + fp > self.budget or len(active) >= self.max_active):
+                with self._used_lock:
+                    used = self.used
+                if active and (used + fp > self.budget or len(active) >= self.max_active):
                     break
                 queue.popleft()
                 r.inst = inst
@@ -196,7 +206,8 @@ class Server:
                     inst.release_tables()          # the engine holds its own copy
                 r.admit_s = time.perf_counter() - t0
                 r.fp = fp
-                self.used += fp
+                with self._used_lock:
+                    self.used += fp
                 active[r.slot] = r
                 if log:
                     log(f"admit {r.rid} n={inst.n_voxel} steps={inst.n_steps} t={r.admit_s:.2f}")
@@ -220,20 +231,54 @@ class Server:
                     r.status = info["status"]
                     work += float(r.inst.n_voxel) * info["step"]
                     # the whole 1 kHz Vm history, to the host (caller order made on the device)
+                    if self.async_download:
+                        import torch
+                        hdev = self.engine.history_device(slot)
+                        torch.cuda.current_stream().synchronize()   # gathered before the instance goes
+                        self.engine.remove(slot)
+                        # its footprint stays booked until the gathered copy is on the host
+                        r.dl_future = self.dl.submit(self._download, r, hdev, keep_history, t0, time_scale, log)
+                        downloading.append(r)
+                        continue
                     hist = self.engine.history_host(slot) if dev_dl else self.engine.history(slot)
                     r.history_bytes = hist.nbytes
                     r.history = hist if keep_history else None
                     r.done_s = time.perf_counter() - t0
                     self.engine.remove(slot)
-                    self.used -= r.fp
+                    with self._used_lock:
+                        self.used -= r.fp
                     done.append(r)
                     if log:
                         log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
+        for r in downloading:
+            r.dl_future.result()
+            done.append(r)
         makespan = time.perf_counter() - t0
         return done, {"makespan_s": makespan, "voxel_steps": work, "launches": self.launches}
 
+    def _download(self, r, hdev, keep_history, t0, time_scale, log):
+        """Worker: copy a retired request's gathered history to the host (its
+        own pinned staging and stream); the request's latency ends here."""
+        from .engine import tensor_to_host
+        import torch
+        tl = self._dl_tls
+        if getattr(tl, "stream", None) is None:
+            tl.stream = torch.cuda.Stream(hdev.device)
+            tl.stage = None
+        hist, tl.stage = tensor_to_host(hdev, tl.stage, stream=tl.stream)
+        del hdev
+        with self._used_lock:
+            self.used -= r.fp
+        r.history_bytes = hist.nbytes
+        r.history = hist if keep_history else None
+        r.done_s = time.perf_counter() - t0
+        if log:
+            log(f"done {r.rid} latency={r.done_s - r.arrival_s * time_scale:.2f}s")
+
     def close(self):
         self.pool.shutdown(wait=True)
+        if self.dl is not None:
+            self.dl.shutdown(wait=True)
         self.engine.close()
 
 
