@@ -76,8 +76,8 @@ def parse():
     p.add_argument("--geometry-only", action="store_true", help="run only the geometry-preparation leg")
     p.add_argument("--plain-only", action="store_true", help="run only the plain-FP64 leg (profiling case)")
     p.add_argument("--serving-only", action="store_true", help="run only the two serving legs")
-    p.add_argument("--serving-sync", action="store_true",
-                   help="retire served requests with a synchronous history download (comparison runs)")
+    p.add_argument("--serving-async", action="store_true",
+                   help="retire served requests with the history copied on a worker thread (comparison runs)")
     return p.parse_args()
 
 
@@ -773,7 +773,7 @@ def serving_leg(args, dev, count=300, compress=20.0, rate=20.0, dur_ms=(200.0, 2
     free = torch.cuda.mem_get_info(dev)[0]
     srv = serving.Server(hbm_budget_bytes=int(free * 0.8), steps_per_launch=100,
                          stream=torch.cuda.current_stream(dev).cuda_stream, device_build=True,
-                         async_download=not args.serving_sync)
+                         async_download=args.serving_async)
     done, totals = srv.run(reqs)
     srv.close()
     out = serving.summarize(done, totals, reqs)
@@ -783,7 +783,7 @@ def serving_leg(args, dev, count=300, compress=20.0, rate=20.0, dur_ms=(200.0, 2
     out["arrival_rate_per_s"] = r_eff
     out["durations_ms"] = list(d)
     out["time_compression"] = compress
-    out["history_download"] = "synchronous" if args.serving_sync else "worker thread, pinned staging, own stream"
+    out["history_download"] = "worker thread, pinned staging, own stream" if args.serving_async else "synchronous"
     if plain_subset:
         by_id = {r.rid: r for r in done}
         sub = sorted(reqs, key=lambda r: r.arrival_s)[:plain_subset]

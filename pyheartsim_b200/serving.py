@@ -12,10 +12,11 @@ between launches,
   persistent launch (instances of different sizes and models share it, each
   with its own team of CTAs, so new requests overlap with running ones);
 * retires instances that reached their last step: gathers the whole 1 kHz Vm
-  history into the caller's voxel order on the device, frees the instance and
-  copies the history to the host on a worker thread through pinned staging
-  buffers on its own stream while the engine keeps running
-  (``async_download``; a request's latency ends when its history is there);
+  history into the caller's voxel order on the device, copies it to the host
+  through pinned staging buffers and frees the instance (a request's latency
+  ends when its history is there).  With ``async_download`` the instance is
+  freed right after the gather and the copy runs on a worker thread on its own
+  stream while the engine keeps running;
 * re-splits CTAs over the running instances by measured cost every
   ``rebalance_every`` launches (the device phase timers run only in the launch
   before each re-split).
@@ -146,7 +147,7 @@ class _Inline:
 class Server:
     def __init__(self, hbm_budget_bytes, steps_per_launch=50, rebalance_every=8, build_threads=8, tol=1e-7,
                  stream=None, engine=None, builder=None, footprint=None, device_build=False, max_active=64,
-                 async_download=True):
+                 async_download=False):
         self.budget = int(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.S = int(steps_per_launch)
