@@ -17,7 +17,8 @@ def _small_requests():
     return reqs
 
 
-def test_result_alone_equals_result_in_the_mix(cuda_device):
+@pytest.mark.parametrize("async_download", [False, True])
+def test_result_alone_equals_result_in_the_mix(async_download, cuda_device):
     alone = {}
     for r in _small_requests():
         srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40)
@@ -29,7 +30,8 @@ def test_result_alone_equals_result_in_the_mix(cuda_device):
     mix[1].arrival_s = 0.002
     mix[2].arrival_s = 0.004
     # built on the device this time: the same instances, so the same results
-    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40, rebalance_every=2, device_build=True)
+    srv = serving.Server(hbm_budget_bytes=8 << 30, steps_per_launch=40, rebalance_every=2, device_build=True,
+                         async_download=async_download)
     done, totals = srv.run(mix, keep_history=True)
     srv.close()
     assert len(done) == 3
