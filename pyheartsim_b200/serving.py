@@ -120,15 +120,18 @@ def build(req, tol=1e-7, restart=20, device=False):
 
 
 def footprint_bytes(inst):
-    """Device bytes of an FP32 instance (tables, state, Krylov basis, history, partials)."""
+    """Device bytes of an FP32 instance (tables incl. the compact neighbour
+    table, state, Krylov basis, partials: per voxel of the length padded to
+    1024 voxels; history: per voxel)."""
     n = inst.n_voxel
+    n_pad = math.ceil(n / 1024) * 1024
     m = min(inst.restart, n)
-    tiles = math.ceil(n / 1024)
+    tiles = math.ceil(n / 512)
     cb = 5 if getattr(inst, "cw", None) is not None else 24
     eb = 72 if getattr(inst, "coef_edge", None) is not None else 0
-    per_voxel = (24 + cb + eb + 1 + 5 * 4 + (m + 1) * 4 + 4 + (4 if inst.guess else 0)
-                 + inst.n_samples * 4 * (2 if inst.save_h else 1))
-    return n * per_voxel + tiles * 8 * (m + 2) * 8 + inst.n_steps + 64 * 1024
+    per_voxel = 24 + 8 + cb + eb + 1 + 5 * 4 + (m + 1) * 4 + 4 + (4 if inst.guess else 0)
+    hist = n * inst.n_samples * 4 * (2 if inst.save_h else 1)
+    return n_pad * per_voxel + hist + tiles * 8 * (m + 2) * 8 + inst.n_steps + 64 * 1024
 
 
 class _Inline:
