@@ -181,3 +181,15 @@ def test_reorder_preserves_the_operator():
     tile = np.arange(n) // 1024
     out = (b.coef6 != 0) & (b.nb6 // 1024 != tile[:, None])
     assert out.sum() / n < 1.0
+
+
+def test_byte_model_closed_forms():
+    """The roofline byte model per voxel-step in FP32 with isotropic rows:
+    71 + 49 k + 4 k^2 with the int32 neighbour table, 55 + 33 k + 4 k^2 (plus
+    the per-block bases, 1/32 byte per row and operator application) with the
+    compact one."""
+    from pyheartsim_b200 import roofline
+    for k in (0, 1, 2, 3, 7):
+        assert roofline.per_voxel_step(4, k) == 71 + 49 * k + 4 * k * k
+        compact = roofline.per_voxel_step(4, k, nb=roofline.COMPACT_NB)
+        assert abs(compact - (55 + 33 * k + 4 * k * k + (1 + k) / 32)) < 1e-9
